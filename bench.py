@@ -1,0 +1,317 @@
+"""Benchmark: lensing maps of the 1000-halo, 4096x4096 workload on B200.
+
+One step = kappa, gamma1, gamma2, mu and the potential (x D_LS/D_OS) of the 4096^2 grid
+over 300"x300" for the seeded 1000-halo catalogue (4 cluster-scale + 996 galaxy-scale
+cut-dPIE halos), computed by the fused lens-maps kernel.  Metric: halo x pixel
+evaluations per second, counting the Hessian and the potential sum once each per
+(halo, pixel) pair.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32c|fp64]
+                  [--impl ours|reference]
+
+--impl reference times the reference's own CPU code (oracle/_ref: gradient2_grid_CPU and
+the reference potential kernel compiled for the host) on all host cores, on a bounded
+band of rows of the same workload.  Multi-GPU (torchrun): independent replicas, one per
+GPU (the maps are independent; no collective on the data path); value = all ranks' evals
+/ max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "maps_1000h_4096"
+METRIC = "halo x pixel evals/s (Hessian + potential, lens maps kappa/gamma1/gamma2/mu/psi)"
+# weighted flop census per pair (fixed convention: +,-,* = 1, fma = 2, div = sqrt = 4,
+# log = atan2 = 20): dPIE Hessian 182 (src/gradient2.cpp:92-167, :54-83) + dPIE potential
+# 760 (src/potential_GPU.cu:47-116 with src/lt_math_GPU.cuh)
+FLOPS_PER_PAIR = 182 + 760
+
+
+def _package():
+    if "lenstool_hpc_b200" in sys.modules:
+        return sys.modules["lenstool_hpc_b200"]
+    pkg_dir = ROOT / "lenstool-hpc_b200"
+    spec = importlib.util.spec_from_file_location("lenstool_hpc_b200", pkg_dir / "__init__.py",
+                                                  submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["lenstool_hpc_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", self.gpu_id], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0., set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = max(mx, float(p[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return json.loads(p.read_text())
+    except Exception:
+        return {}
+
+
+def reference_cpu(steps, warmup, rows=None):
+    """Reference CPU code on a band of rows of the workload; returns (evals/s, info)."""
+    import oracle
+    lt = _package()
+    from lenstool_hpc_b200 import catalog
+    ref = oracle.RefLib()
+    cat, g = catalog.workload(WORKLOAD)
+    threads = os.cpu_count()
+    rows = rows or max(1, min(64, threads // 4))
+    band = catalog.Grid(g.xmin, g.xmax, g.ymin, g.ymax, g.nx, rows, 0, g.ny // 2, dx=g.dx, dy=g.dy)
+    times = []
+    for it in range(warmup + steps):
+        t0 = time.perf_counter()
+        ref.hess_grid(cat, band)
+        px, py = band.coords()
+        ref.pot81_points(cat, px, py)
+        dt = time.perf_counter() - t0
+        if it >= warmup:
+            times.append(dt)
+    evals = 2 * band.npix * cat.n
+    v = evals / float(np.mean(times))
+    sample = (f"{rows} rows x {g.nx} px x {cat.n} halos of the workload (gradient2_grid_CPU + reference potential "
+              f"kernel on the host), {threads} OpenMP threads")
+    return v, {"value": v, "unit": "evals/s", "cores": threads, "kind": "reference", "sample": sample,
+               "seconds_per_sample": float(np.mean(times))}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    warmup = max(args.warmup, 3)
+    rank, local_rank, world = dist_env()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v, info = reference_cpu(args.steps, warmup)
+        line = {"metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": warmup, "ms_per_step": 1e3 * info["seconds_per_sample"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference", "config": {"workload": WORKLOAD, "sample": info["sample"]},
+                "cpu_baseline": info, "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                                              "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    lt = _package()
+    from lenstool_hpc_b200 import build, catalog
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    build.build()
+    cat, g = catalog.workload(WORKLOAD)
+    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
+    D = dls / dos
+    ctx = lt.Context(local_rank)
+    dcat = ctx.upload(cat)
+    stream = torch.cuda.Stream()
+    names = ("kappa", "gamma1", "gamma2", "mu", "psi")
+    outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in names}
+
+    def step():
+        ctx.lens_maps(dcat, g, precision=args.precision, dlsds=D, out=outs, stream=stream)
+
+    for _ in range(warmup):
+        step()
+    ctx.synchronize(stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    props = torch.cuda.get_device_properties(local_rank)
+    gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    t_all0 = torch.cuda.Event(enable_timing=True)
+    t_all1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    n0 = lt.launch_count()
+    with ClockSampler(gpu_id) as clocks:
+        t_all0.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            step()
+            ends[k].record(stream)
+        t_all1.record(stream)
+        ctx.synchronize(stream)
+        barrier()
+    launches = lt.launch_count() - n0
+    elapsed = t_all0.elapsed_time(t_all1) / 1e3
+    per_launch = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)])) / 1e3
+    tmax = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+    elapsed = float(tmax.item())
+    evals_step = 2 * g.npix * cat.n
+    value = world * evals_step * args.steps / elapsed
+
+    # end to end through the public API with host buffers: catalogue upload from host
+    # arrays and the maps copied back into pinned host memory, every step
+    e2e = None
+    if not args.no_e2e:
+        host = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, pin_memory=True) for k in names}
+        hnp = {k: v.numpy() for k, v in host.items()}
+        for _ in range(1):
+            c2 = ctx.upload(cat)
+            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp)
+            c2.release()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            c2 = ctx.upload(cat)
+            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp)
+            c2.release()
+        torch.cuda.synchronize()
+        te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        h2d = 192 * cat.n + 16 * cat.n
+        d2h = len(names) * g.npix * 8
+        e2e = {"value": world * evals_step * args.steps / float(te.item()), "unit": "evals/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "note": "host SoA -> lt_catalog_upload (packed records + chunk table) and 5 float64 maps -> pinned host"}
+
+    if rank == 0:
+        peaks = measured_peaks()
+        pipe = "fp64" if args.precision == "fp64" else "fp32"
+        peak_tflops = fma_peak_tflops(pipe)
+        achieved = evals_step * FLOPS_PER_PAIR / 2 / per_launch / 1e12
+        out_bytes = len(names) * g.npix * 8
+        cpu = None
+        if not args.no_cpu_baseline:
+            try:
+                _, cpu = reference_cpu(1, 1)
+            except Exception as ex:  # the reference library is absent
+                cpu = {"value": None, "unit": "evals/s", "kind": "reference", "cores": os.cpu_count(),
+                       "sample": f"unavailable: {ex}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": f"{g.nx}x{g.ny} over 300\"x300\"", "halos": cat.n,
+                       "maps": list(names), "precision": args.precision, "evals_per_step": evals_step,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "outputs 671 MB per step > 126 MB L2; catalogue 192 KB stays resident"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                         "frac": achieved / peak_tflops if peak_tflops else None, "traffic": None,
+                         "kernel": f"lt::grid64_kernel<OP_HESS|OP_POT>" if args.precision == "fp64" else
+                         "lt::grid32c_kernel",
+                         "flops_per_pair": FLOPS_PER_PAIR, "flop_convention": "weighted census, FMA-equivalents",
+                         "peak_source": f"measured in-run: {pipe} FMA-chain kernel",
+                         "hbm_writeback_gbs": out_bytes / per_launch / 1e9,
+                         "hbm_peak_gbs": peaks.get("hbm_gbs")},
+            "clocks": clocks.summary(),
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def fma_peak_tflops(pipe: str) -> float:
+    """Measured FMA throughput of this GPU (TFLOP/s, FMA = 2 flops) from the library's
+    FMA-chain kernel."""
+    lt = _package()
+    L = lt.load_library()
+    fn = getattr(L, "lt_measure_fma_peak", None)
+    if fn is None:
+        return None
+    fn.restype = C.c_double
+    fn.argtypes = [C.c_int, C.c_int]
+    return float(fn(0 if pipe == "fp64" else 1, 0))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,181 @@
+/*
+ * lt_b200.h -- C ABI of the B200 lensing-map library (liblt_b200.so).
+ *
+ * The library evaluates Lenstool-HPC's per-pixel sum over halos of the lens-potential
+ * gradient (deflection), Hessian and potential for the SIS (type 5), PIEMD (type 8) and
+ * cut dPIE (type 81) profiles, and the maps built on them, on one NVIDIA B200.
+ *
+ * Conventions shared by every entry point
+ *   - Plain C types only; every call returns an lt_status and never exits the process.
+ *   - A catalogue is uploaded once (lt_catalog_upload) and stays resident in HBM; the
+ *     grid calls take the handle.  The halo fields keep the meaning of the reference's
+ *     struct Potential_SOA (src/structure_hpc.hpp:257-287).
+ *   - Output planes are float64, row-major nx*ny, pixel (i, j) at
+ *     x = xmin + (i + istart) dx, y = ymin + (j + jstart) dy and index j*nx + i
+ *     (src/grid_gradient_CPU.cpp:67-100).
+ *   - Output pointers may be device pointers (the call is then asynchronous on `stream`)
+ *     or host pointers (the library stages through device memory, copies back and
+ *     synchronises `stream` before returning, like the reference's host wrappers).
+ *   - `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream.
+ *   - Precision: LT_FP64 reproduces the reference FP64 CPU path to <= 1e-12 (relative
+ *     to max(|value|, RMS of the map)); LT_FP32C runs the bulk halo sum in FP32 with
+ *     compensated accumulation and keeps FP64 for cluster-scale halos, near-core pairs and
+ *     pixels near critical curves (the error against FP64 is reported by the tests).
+ */
+#ifndef LT_B200_H
+#define LT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LT_B200_ABI_VERSION 1
+
+typedef enum {
+    LT_OK = 0,
+    LT_ERR_INVALID_ARGUMENT = 1,   /* NULL pointer, bad size, bad grid, bad map kind */
+    LT_ERR_UNKNOWN_PROFILE = 2,    /* halo type other than 5, 8, 81 */
+    LT_ERR_NONFINITE = 3,          /* NaN/Inf or out-of-domain halo parameter */
+    LT_ERR_CUDA = 4,               /* a CUDA runtime call failed (see lt_last_error) */
+    LT_ERR_OUT_OF_MEMORY = 5,      /* device allocation failed */
+    LT_ERR_BUDGET = 6,             /* the context's HBM budget would be exceeded */
+    LT_ERR_QUEUE_FULL = 7,         /* serving queue has no free slot */
+    LT_ERR_TIMEOUT = 8,            /* a bounded device-side wait gave up */
+    LT_ERR_NO_DEVICE = 9,          /* no CUDA device / wrong architecture */
+    LT_ERR_NOT_READY = 10          /* asynchronous result not yet available */
+} lt_status;
+
+typedef enum { LT_FP64 = 0, LT_FP32C = 1 } lt_precision;
+
+/* Map kinds computed from the Hessian [[a, b], [d, c]] with D = dlsds (D_LS/D_OS).
+ * Reference kernels: ampli src/grid_map_ampli_GPU.cu:329-547, shear
+ * src/grid_map_shear_GPU.cu:208-369, mass src/grid_map_mass_GPU.cu:307-322. */
+typedef enum {
+    LT_MAP_HESS_A = 0, LT_MAP_HESS_B = 1, LT_MAP_HESS_C = 2, LT_MAP_HESS_D = 3, /* raw planes */
+    LT_MAP_AMPLI1 = 11,  /* 1/(lambda mu) of A = 1 - aD, B = -bD, C = 1 - cD            */
+    LT_MAP_AMPLI2 = 12,  /* 1/|lambda mu|                                              */
+    LT_MAP_AMPLI3 = 13,  /* -2.5 log10 |lambda mu|                                     */
+    LT_MAP_AMPLI4 = 14,  /* (1-k)(1+gp^2)/(1-gp^2), gp = |g|/(1-k)                      */
+    LT_MAP_AMPLI5 = 15,  /* (a + c)/2, not scaled by D (as the reference)              */
+    LT_MAP_AMPLI6 = 16,  /* sqrt(((a-c)/2)^2 + b^2), not scaled by D                   */
+    LT_MAP_SHEAR1 = 21,  /* (lambda - mu)/2                                            */
+    LT_MAP_SHEAR2 = 22,  /* |(q^2-1)/(q^2+1)|, q = lambda/mu                           */
+    LT_MAP_SHEAR3 = 23,  /* gamma1 = (a - c) D/2                                       */
+    LT_MAP_SHEAR4 = 24,  /* gamma2 = b D                                               */
+    LT_MAP_KAPPA = 31,   /* kappa = (a + c) D/2                                        */
+    LT_MAP_GAMMA1 = 32,  /* (a - c) D/2                                                */
+    LT_MAP_GAMMA2 = 33,  /* b D                                                        */
+    LT_MAP_MU = 34,      /* 1/((1-kappa)^2 - gamma1^2 - gamma2^2), determinant in FP64 */
+    LT_MAP_MASS = 41     /* (a + c)/2 * mult (Kmap Hessian; mult per mass mode)        */
+} lt_map_kind;
+
+#define LT_MAX_MAPS 8
+
+/* Halo catalogue, host arrays of nhalos entries (Potential_SOA fields used by the path). */
+typedef struct {
+    int32_t nhalos;
+    const int32_t *type;                  /* 5, 8 or 81                                 */
+    const double *position_x, *position_y;/* arcsec                                     */
+    const double *b0;                     /* impact parameter                           */
+    const double *anglecos, *anglesin;    /* cos/sin of ellipticity_angle               */
+    const double *ellipticity_potential;  /* in (0, 1)                                  */
+    const double *rcore, *rcut;           /* arcsec (rcut > rcore for type 81)          */
+    const double *dlsds;                  /* per-halo D_LS/D_OS for Kmap; NULL = all 1  */
+} lt_halo_soa;
+
+typedef struct {
+    double xmin, ymin, dx, dy;
+    int32_t nx, ny, istart, jstart;
+} lt_grid;
+
+typedef struct {
+    int32_t kind;    /* lt_map_kind */
+    double *out;     /* nx*ny float64, host or device */
+} lt_map_request;
+
+typedef struct {
+    int32_t model;   /* 1 (CPL dark energy), src/module_cosmodistances.cpp:222-230 */
+    double omegaM, omegaX, curvature, wX, wa, H0;
+} lt_cosmology;
+
+typedef struct lt_context lt_context;
+typedef struct lt_catalog lt_catalog;
+
+/* ---- context and catalogues ------------------------------------------------------ */
+
+/* Create a context on CUDA device `device`.  hbm_budget_bytes caps the device memory the
+ * context may hold (0 = 90% of free memory at creation).  No counterpart in the reference
+ * (its wrappers allocate and free on every call, src/grid_gradient_GPU.cu:94-178). */
+lt_status lt_create(int device, size_t hbm_budget_bytes, lt_context **ctx);
+lt_status lt_destroy(lt_context *ctx);
+
+/* Validate and pack a catalogue into HBM.  Replaces the per-call cudaMalloc/cudaMemcpy of
+ * the reference wrappers (src/grid_map_ampli_GPU.cu:119-160). */
+lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *soa, lt_catalog **cat);
+lt_status lt_catalog_release(lt_context *ctx, lt_catalog *cat);
+int32_t lt_catalog_nhalos(const lt_catalog *cat);
+
+/* ---- grid evaluators ------------------------------------------------------------- */
+
+/* Deflection grid, both planes multiplied by `scale` (1 for the raw gradient, D_LS/D_OS
+ * for a displacement map).  Replaces gradient_grid_CPU/GPU (src/grid_gradient_CPU.cpp:56,
+ * src/grid_gradient_GPU.cu:77-179), module_potentialDerivatives_totalGradient_SOA_CPU_GPU
+ * (src/grid_gradient_GPU.cuh:40-41) and map_grid_dpl_GPU (src/grid_map_dpl_GPU.cu:75-173). */
+lt_status lt_gradient_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                           double scale, double *ax, double *ay, void *stream);
+
+/* Hessian grid and up to LT_MAX_MAPS derived maps in one pass.  kmap != 0 weights every
+ * halo by its dlsds (module_potentialDerivatives_Kmap_SOA_GPU, src/gradient2_GPU.cu:455-522).
+ * Replaces gradient2_grid_CPU/GPU (src/grid_gradient2_CPU.cpp:54-83,
+ * src/grid_gradient2_GPU.cu:77-183) and map_grid_{ampli,shear,mass}_GPU
+ * (src/grid_map_ampli_GPU.cu:93-192, src/grid_map_shear_GPU.cu:87-187,
+ * src/grid_map_mass_GPU.cu:82-216). */
+lt_status lt_hessian_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                          int32_t kmap, double dlsds, double mult, const lt_map_request *maps, int32_t nmaps,
+                          void *stream);
+
+/* Potential grid multiplied by `scale` (D_LS/D_OS for potential mode 1, cH2piG h / D_OL
+ * for mode 2).  Replaces potential_grid_GPU / module_potential_SOA_CPU_GPU
+ * (src/grid_potential_GPU.cu:68-184) and map_grid_potential_GPU
+ * (src/grid_map_pot_GPU.cu:83-273). */
+lt_status lt_potential_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                            double scale, double *psi, void *stream);
+
+/* All configuration-1 maps of one grid in one fused pass: kappa, gamma1, gamma2, mu (as
+ * LT_MAP_*), and the potential scaled by D (any output may be NULL). */
+lt_status lt_lens_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                       double dlsds, double *kappa, double *gamma1, double *gamma2, double *mu, double *psi,
+                       void *stream);
+
+/* Wait for the context's work on `stream` and report any status a kernel recorded
+ * (e.g. LT_ERR_TIMEOUT from a bounded device-side wait).  Asynchronous (device-pointer)
+ * calls report such errors here. */
+lt_status lt_synchronize(lt_context *ctx, void *stream);
+
+/* ---- cosmology and utilities ----------------------------------------------------- */
+
+/* D_LS, D_OS, D_OL in units of c/H0 (module_cosmodistances_objectObject/observerObject,
+ * src/module_cosmodistances.cpp:94-151).  Host only; needs no GPU. */
+lt_status lt_cosmo_distances(const lt_cosmology *cosmo, double zl, double zs, double *dls, double *dos,
+                             double *dol);
+
+/* Number of kernels this library has launched in the calling process (all contexts). */
+uint64_t lt_kernel_launch_count(void);
+
+/* Measured FMA-pipe throughput of `device` in TFLOP/s (an FMA counts 2 flops), FP64
+ * (fp32 = 0) or FP32 (fp32 = 1); 0 on failure.  A measurement utility with no
+ * counterpart in the reference: the denominator of the grid kernels' roofline. */
+double lt_measure_fma_peak(int fp32, int device);
+
+const char *lt_status_string(lt_status status);
+/* Last error message recorded by the context (never NULL). */
+const char *lt_last_error(const lt_context *ctx);
+int32_t lt_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LT_B200_H */

@@ -1,0 +1,366 @@
+"""lenstool-hpc_b200 -- B200-native lensing-map hot path of Lenstool-HPC.
+
+Python host mirror of the C ABI in include/lt_b200.h (library liblt_b200.so built by
+build.py).  There is no CPU fallback: every call runs the CUDA kernels, and importing the
+bindings fails loudly when the library is missing.
+
+Reference-named wrappers at the bottom (gradient_grid_GPU, gradient2_grid_GPU,
+map_grid_ampli_GPU, ...) take the same arguments as the reference's host functions
+(src/grid_gradient_GPU.cuh:34-36, src/grid_gradient2_GPU.cuh:32-34,
+src/grid_map_*_GPU.cuh) with a HaloCatalog in place of Potential_SOA.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+import numpy as np
+
+from . import catalog, cosmo  # noqa: F401
+from .catalog import Grid, HaloCatalog  # noqa: F401
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "liblt_b200.so"
+
+# lt_status
+STATUS = {0: "LT_OK", 1: "LT_ERR_INVALID_ARGUMENT", 2: "LT_ERR_UNKNOWN_PROFILE", 3: "LT_ERR_NONFINITE",
+          4: "LT_ERR_CUDA", 5: "LT_ERR_OUT_OF_MEMORY", 6: "LT_ERR_BUDGET", 7: "LT_ERR_QUEUE_FULL",
+          8: "LT_ERR_TIMEOUT", 9: "LT_ERR_NO_DEVICE", 10: "LT_ERR_NOT_READY"}
+FP64, FP32C = 0, 1
+PRECISION = {"fp64": FP64, "fp32c": FP32C, FP64: FP64, FP32C: FP32C}
+
+# lt_map_kind
+MAP = {"hess_a": 0, "hess_b": 1, "hess_c": 2, "hess_d": 3,
+       "ampli1": 11, "ampli2": 12, "ampli3": 13, "ampli4": 14, "ampli5": 15, "ampli6": 16,
+       "shear1": 21, "shear2": 22, "shear3": 23, "shear4": 24,
+       "kappa": 31, "gamma1": 32, "gamma2": 33, "mu": 34, "mass": 41}
+MAX_MAPS = 8
+
+# physical constants of src/structure_hpc.hpp:62-73
+CH2PIG = 0.11585881
+CH4PIG = 0.057929405
+CH0_4PIG = 2.7730112e-4
+MCRIT12 = .2343165
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+
+
+class LensError(RuntimeError):
+    def __init__(self, status: int, message: str = ""):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        super().__init__(f"{self.name}: {message}" if message else self.name)
+
+
+class _Soa(C.Structure):
+    _fields_ = [("nhalos", C.c_int32), ("type", _ip)] + [(f, _dp) for f in (
+        "position_x", "position_y", "b0", "anglecos", "anglesin", "ellipticity_potential", "rcore", "rcut",
+        "dlsds")]
+
+
+class _Grid(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("ymin", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+                ("nx", C.c_int32), ("ny", C.c_int32), ("istart", C.c_int32), ("jstart", C.c_int32)]
+
+
+class _MapReq(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("out", C.c_void_p)]
+
+
+class _Cosmo(C.Structure):
+    _fields_ = [("model", C.c_int32), ("omegaM", C.c_double), ("omegaX", C.c_double), ("curvature", C.c_double),
+                ("wX", C.c_double), ("wa", C.c_double), ("H0", C.c_double)]
+
+
+_LIB = None
+
+# every symbol the C ABI exports (include/lt_b200.h)
+EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release", "lt_catalog_nhalos",
+           "lt_gradient_grid", "lt_hessian_maps", "lt_potential_grid", "lt_lens_maps", "lt_synchronize",
+           "lt_cosmo_distances", "lt_kernel_launch_count", "lt_status_string", "lt_last_error", "lt_abi_version")
+
+
+def load_library(path=None):
+    """Load liblt_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    p = pathlib.Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: build it with `python lenstool-hpc_b200/build.py`")
+    L = C.CDLL(str(p))
+    vp = C.c_void_p
+    L.lt_create.argtypes = [C.c_int, C.c_size_t, C.POINTER(vp)]
+    L.lt_destroy.argtypes = [vp]
+    L.lt_catalog_upload.argtypes = [vp, C.POINTER(_Soa), C.POINTER(vp)]
+    L.lt_catalog_release.argtypes = [vp, vp]
+    L.lt_catalog_nhalos.argtypes = [vp]
+    L.lt_gradient_grid.argtypes = [vp, vp, C.POINTER(_Grid), C.c_int32, C.c_double, vp, vp, vp]
+    L.lt_hessian_maps.argtypes = [vp, vp, C.POINTER(_Grid), C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                  C.POINTER(_MapReq), C.c_int32, vp]
+    L.lt_potential_grid.argtypes = [vp, vp, C.POINTER(_Grid), C.c_int32, C.c_double, vp, vp]
+    L.lt_lens_maps.argtypes = [vp, vp, C.POINTER(_Grid), C.c_int32, C.c_double, vp, vp, vp, vp, vp, vp]
+    L.lt_synchronize.argtypes = [vp, vp]
+    L.lt_cosmo_distances.argtypes = [C.POINTER(_Cosmo), C.c_double, C.c_double, _dp, _dp, _dp]
+    L.lt_kernel_launch_count.restype = C.c_uint64
+    L.lt_status_string.restype = C.c_char_p
+    L.lt_status_string.argtypes = [C.c_int]
+    L.lt_last_error.restype = C.c_char_p
+    L.lt_last_error.argtypes = [vp]
+    if path is None:
+        _LIB = L
+    return L
+
+
+def launch_count() -> int:
+    """Kernels launched by the library in this process."""
+    return int(load_library().lt_kernel_launch_count())
+
+
+def cosmo_distances(zl: float, zs: float, cosmology: "cosmo.Cosmology | None" = None):
+    """(D_LS, D_OS, D_OL) in units of c/H0, computed by the library (host only)."""
+    c = cosmology or cosmo.Cosmology()
+    s = _Cosmo(c.model, c.omegaM, c.omegaX, c.curvature, c.wX, c.wa, c.H0)
+    a, b, d = C.c_double(), C.c_double(), C.c_double()
+    st = load_library().lt_cosmo_distances(C.byref(s), zl, zs, C.byref(a), C.byref(b), C.byref(d))
+    if st:
+        raise LensError(st, "cosmology")
+    return a.value, b.value, d.value
+
+
+def _grid(g: Grid) -> _Grid:
+    return _Grid(g.xmin, g.ymin, g.dx, g.dy, g.nx, g.ny, g.istart, g.jstart)
+
+
+def _ptr(x):
+    """(address, keep-alive) of a numpy array or a torch tensor."""
+    if isinstance(x, np.ndarray):
+        if x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise ValueError("output arrays must be C-contiguous float64")
+        return x.ctypes.data
+    if hasattr(x, "data_ptr"):
+        if str(x.dtype) != "torch.float64" or not x.is_contiguous():
+            raise ValueError("output tensors must be contiguous float64")
+        return x.data_ptr()
+    raise TypeError(f"unsupported output type {type(x)}")
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    if hasattr(stream, "cuda_stream"):
+        return stream.cuda_stream
+    return int(stream)
+
+
+class Catalog:
+    """A catalogue resident in HBM (lt_catalog handle)."""
+
+    def __init__(self, ctx: "Context", handle, nhalos: int, source: HaloCatalog):
+        self.ctx, self.handle, self.nhalos, self.source = ctx, handle, nhalos, source
+
+    def release(self):
+        if self.handle:
+            self.ctx._lib.lt_catalog_release(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+class Context:
+    """lt_context: one device, an HBM budget, resident catalogues."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        st = self._lib.lt_create(device, budget_bytes, C.byref(h))
+        if st:
+            raise LensError(st, "lt_create")
+        self.handle = h
+
+    def close(self):
+        if self.handle:
+            self._lib.lt_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st, what):
+        if st:
+            msg = self._lib.lt_last_error(self.handle).decode()
+            raise LensError(st, f"{what}: {msg}")
+
+    def upload(self, cat: HaloCatalog) -> Catalog:
+        c = cat.contiguous()
+        keep = c.arrays()
+        d = lambda a: a.ctypes.data_as(_dp)  # noqa: E731
+        s = _Soa(c.n, c.type.ctypes.data_as(_ip), d(c.position_x), d(c.position_y), d(c.b0), d(c.anglecos),
+                 d(c.anglesin), d(c.ellipticity_potential), d(c.rcore), d(c.rcut), d(c.dlsds))
+        h = C.c_void_p()
+        st = self._lib.lt_catalog_upload(self.handle, C.byref(s), C.byref(h))
+        del keep
+        self._check(st, "lt_catalog_upload")
+        return Catalog(self, h, c.n, c)
+
+    def _cat(self, cat):
+        return cat if isinstance(cat, Catalog) else self.upload(cat)
+
+    @staticmethod
+    def _outs(grid: Grid, out, n):
+        if out is None:
+            return [np.empty((grid.ny, grid.nx)) for _ in range(n)]
+        return list(out)
+
+    def gradient_grid(self, cat, grid: Grid, precision="fp64", scale=1.0, out=None, stream=None):
+        cat = self._cat(cat)
+        ax, ay = self._outs(grid, out, 2)
+        st = self._lib.lt_gradient_grid(self.handle, cat.handle, C.byref(_grid(grid)), PRECISION[precision], scale,
+                                        _ptr(ax), _ptr(ay), _stream_handle(stream))
+        self._check(st, "lt_gradient_grid")
+        return ax, ay
+
+    def hessian_maps(self, cat, grid: Grid, kinds, precision="fp64", kmap=False, dlsds=1.0, mult=1.0, out=None,
+                     stream=None):
+        cat = self._cat(cat)
+        kinds = list(kinds)
+        outs = self._outs(grid, out, len(kinds))
+        req = (_MapReq * len(kinds))(*[_MapReq(MAP[k] if isinstance(k, str) else int(k), _ptr(o))
+                                       for k, o in zip(kinds, outs)])
+        st = self._lib.lt_hessian_maps(self.handle, cat.handle, C.byref(_grid(grid)), PRECISION[precision],
+                                       int(bool(kmap)), dlsds, mult, req, len(kinds), _stream_handle(stream))
+        self._check(st, "lt_hessian_maps")
+        return dict(zip(kinds, outs))
+
+    def potential_grid(self, cat, grid: Grid, precision="fp64", scale=1.0, out=None, stream=None):
+        cat = self._cat(cat)
+        (psi,) = self._outs(grid, None if out is None else [out], 1)
+        st = self._lib.lt_potential_grid(self.handle, cat.handle, C.byref(_grid(grid)), PRECISION[precision], scale,
+                                         _ptr(psi), _stream_handle(stream))
+        self._check(st, "lt_potential_grid")
+        return psi
+
+    def lens_maps(self, cat, grid: Grid, precision="fp64", dlsds=1.0, out=None, stream=None,
+                  which=("kappa", "gamma1", "gamma2", "mu", "psi")):
+        """kappa, gamma1, gamma2, mu and psi*dlsds of one grid in one fused pass."""
+        cat = self._cat(cat)
+        names = ("kappa", "gamma1", "gamma2", "mu", "psi")
+        if out is None:
+            out = {k: np.empty((grid.ny, grid.nx)) for k in which}
+        ptrs = [(_ptr(out[k]) if k in out else None) for k in names]
+        st = self._lib.lt_lens_maps(self.handle, cat.handle, C.byref(_grid(grid)), PRECISION[precision], dlsds,
+                                    *ptrs, _stream_handle(stream))
+        self._check(st, "lt_lens_maps")
+        return out
+
+    def synchronize(self, stream=None):
+        self._check(self._lib.lt_synchronize(self.handle, _stream_handle(stream)), "lt_synchronize")
+
+
+# ---------------------------------------------------------------------------------------
+# Reference-named entry points (same argument meaning as the reference's host wrappers).
+# ---------------------------------------------------------------------------------------
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def _frame_grid(frame, nbgridcells, nx=None, ny=None, dx=None, dy=None, istart=0, jstart=0) -> Grid:
+    nx = nx or nbgridcells
+    ny = ny or nbgridcells
+    g = Grid(frame["xmin"], frame["xmax"], frame["ymin"], frame["ymax"], nx, ny, istart, jstart)
+    if dx is not None:
+        g.dx, g.dy = dx, dy
+    return g
+
+
+def gradient_grid_GPU(frame, lens: HaloCatalog, nbgridcells, **kw):
+    """src/grid_gradient_GPU.cu:77-84: (grid_grad_x, grid_grad_y) over a square grid."""
+    return default_context().gradient_grid(lens, _frame_grid(frame, nbgridcells, **kw))
+
+
+def gradient2_grid_GPU(frame, lens: HaloCatalog, nbgridcells, **kw):
+    """src/grid_gradient2_GPU.cu:77-183: the four Hessian planes (a, b, c, d)."""
+    m = default_context().hessian_maps(lens, _frame_grid(frame, nbgridcells, **kw),
+                                       ["hess_a", "hess_b", "hess_c", "hess_d"])
+    return m["hess_a"], m["hess_b"], m["hess_c"], m["hess_d"]
+
+
+def map_grid_ampli_GPU(mode, cosmology, frame, lens: HaloCatalog, nbgridcells, z, **kw):
+    """src/grid_map_ampli_GPU.cu:93-192: amplification map mode 1-6 for sources at z."""
+    if mode not in range(1, 7):
+        raise LensError(1, f"amplification mode {mode} not supported")
+    dls, dos, _ = cosmo_distances(lens.z, z, cosmology)
+    k = f"ampli{mode}"
+    return default_context().hessian_maps(lens, _frame_grid(frame, nbgridcells, **kw), [k], dlsds=dls / dos)[k]
+
+
+def map_grid_shear_GPU(mode, cosmology, frame, lens: HaloCatalog, nbgridcells, z, **kw):
+    """src/grid_map_shear_GPU.cu:87-187: shear map mode 1-4."""
+    if mode not in range(1, 5):
+        raise LensError(1, f"shear mode {mode} not supported")
+    dls, dos, _ = cosmo_distances(lens.z, z, cosmology)
+    k = f"shear{mode}"
+    return default_context().hessian_maps(lens, _frame_grid(frame, nbgridcells, **kw), [k], dlsds=dls / dos)[k]
+
+
+def mass_multiplier(mode, dl0s, ds, dl, h, dx, dy):
+    """Unit factor of mass map modes 1-4 (src/grid_map_mass_GPU.cu:219-300)."""
+    if mode == 1:
+        return 1.
+    if mode == 2:
+        return CH4PIG * h / dl / dl0s * ds
+    if mode == 3:
+        return MCRIT12 / h * dx * dy * dl / dl0s * ds
+    if mode == 4:
+        return CH0_4PIG * h / dl / dl0s * ds
+    raise LensError(1, f"mass mode {mode} not supported")
+
+
+def map_grid_mass_GPU(mode, cosmology, frame, lens: HaloCatalog, nbgridcells, zl, zs, **kw):
+    """src/grid_map_mass_GPU.cu:82-216: Kmap (per-halo dlsds weights) times the mode's unit."""
+    c = cosmology or cosmo.Cosmology()
+    zl = zl or lens.z
+    dl0s, ds, dl = cosmo_distances(zl, zs, c)
+    g = _frame_grid(frame, nbgridcells, **kw)
+    mult = mass_multiplier(mode, dl0s, ds, dl, c.h, g.dx, g.dy)
+    return default_context().hessian_maps(lens, g, ["mass"], kmap=True, mult=mult)["mass"]
+
+
+def map_grid_potential_GPU(mode, cosmology, frame, lens: HaloCatalog, nbgridcells, z, **kw):
+    """src/grid_map_pot_GPU.cu:83-273: potential mode 1 (x D_LS/D_OS) or 2 (x cH2piG h/D_OL)."""
+    c = cosmology or cosmo.Cosmology()
+    dl0s, ds, dl = cosmo_distances(lens.z, z, c)
+    if mode == 1:
+        scale = dl0s / ds
+    elif mode == 2:
+        scale = CH2PIG * c.h / dl
+    else:
+        raise LensError(1, f"potential mode {mode} not supported")
+    return default_context().potential_grid(lens, _frame_grid(frame, nbgridcells, **kw), scale=scale)
+
+
+def map_grid_dpl_GPU(cosmology, frame, lens: HaloCatalog, nbgridcells, z, **kw):
+    """src/grid_map_dpl_GPU.cu:75-173: deflection x D_LS/D_OS, two planes."""
+    dl0s, ds, _ = cosmo_distances(lens.z, z, cosmology)
+    return default_context().gradient_grid(lens, _frame_grid(frame, nbgridcells, **kw), scale=dl0s / ds)

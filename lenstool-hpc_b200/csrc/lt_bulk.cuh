@@ -1,0 +1,157 @@
+/*
+ * lt_bulk.cuh -- shared-memory staging of halo tiles with the Blackwell bulk-copy
+ * engine (cp.async.bulk, global -> shared, completion on an mbarrier), and the map
+ * epilogue shared by the grid kernels.
+ *
+ * Every wait on an mbarrier is bounded: after LT_WAIT_LIMIT polls the kernel records
+ * LT_ERR_TIMEOUT in its status word and the block leaves together (see wait_tile).
+ */
+#pragma once
+#include <stdint.h>
+#include "lt_grid.cuh"
+
+#define LT_WAIT_LIMIT (1u << 24)
+
+namespace lt {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+/* Arrive once and announce `bytes` of incoming transactions. */
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+/* Bulk copy of `bytes` (multiple of 16, both addresses 16-byte aligned) from global to
+ * this CTA's shared memory, completing on `bar`.  No multicast. */
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+/* Bounded wait of the whole block for phase `parity` of `bar`.  Returns false (after
+ * recording LT_ERR_TIMEOUT) when any thread gave up; every thread of the block takes
+ * the same branch because the outcome is reduced with __syncthreads_or. */
+__device__ __forceinline__ bool wait_tile(uint64_t *bar, uint32_t parity, int32_t *status)
+{
+    int gave_up = 0;
+    uint32_t tries = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++tries > LT_WAIT_LIMIT) {
+            gave_up = 1;
+            break;
+        }
+    }
+    if (__syncthreads_or(gave_up)) {
+        if (threadIdx.x == 0 && status) atomicExch(status, (int32_t)LT_ERR_TIMEOUT);
+        return false;
+    }
+    return true;
+}
+
+/* Before leaving after a timeout, let a copy still in flight land (bounded). */
+__device__ __forceinline__ void drain_tile(uint64_t *bar, uint32_t parity)
+{
+    uint32_t tries = 0;
+    while (!mbar_try_wait(bar, parity) && ++tries < LT_WAIT_LIMIT) {
+    }
+}
+
+/* Coordinates of pixel column i / row j without a fused multiply-add, so that they equal
+ * the reference's xmin + (i + istart) dx bit for bit. */
+__device__ __forceinline__ double pixel_x(const GridArgs &a, int i)
+{
+    return __dadd_rn(a.xmin, __dmul_rn((double)(i + a.istart), a.dx));
+}
+__device__ __forceinline__ double pixel_y(const GridArgs &a, int j)
+{
+    return __dadd_rn(a.ymin, __dmul_rn((double)(j + a.jstart), a.dy));
+}
+
+/* Eigenvalues of [[A, B], [B, C]] (formeli_ampli, src/grid_map_ampli_GPU.cu:549-572). */
+__device__ __forceinline__ void eigen2(double A, double B, double C, double &lam, double &mu)
+{
+    double delta = (A - C) * (A - C) + 4. * B * B;
+    double e = sqrt(delta);
+    lam = .5 * (A + C + e);
+    mu = .5 * (A + C - e);
+}
+
+/* Value of one output plane at one pixel from the pixel's sums. */
+__device__ __forceinline__ double map_value(int kind, double gx, double gy, double hxx, double hyy, double hxy,
+                                            double psi, double D, double mult, double scale)
+{
+    double a = hxx, b = hxy, c = hyy;
+    double lam, mu;
+    switch (kind) {
+    case LT_MAP_HESS_A: return a;
+    case LT_MAP_HESS_B: return b;
+    case LT_MAP_HESS_C: return c;
+    case LT_MAP_HESS_D: return b;
+    case LT_MAP_AMPLI1: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return 1. / (lam * mu);
+    case LT_MAP_AMPLI2: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return 1. / fabs(lam * mu);
+    case LT_MAP_AMPLI3: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return -2.5 * log10(fabs(lam * mu));
+    case LT_MAP_AMPLI4: {
+        double k = (a + c) * D / 2.;
+        double g1 = (a - c) * D / 2.;
+        double g2 = b * D;
+        double g = sqrt(g1 * g1 + g2 * g2);
+        double gp = g / (1 - k);
+        return (1 - k) * (1 + gp * gp) / (1 - gp * gp);
+    }
+    case LT_MAP_AMPLI5: return (a + c) / 2.;
+    case LT_MAP_AMPLI6: {
+        double g1 = (a - c) / 2.;
+        return sqrt(g1 * g1 + b * b);
+    }
+    case LT_MAP_SHEAR1: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return (lam - mu) / 2.;
+    case LT_MAP_SHEAR2: {
+        eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu);
+        double q = lam / mu;
+        return fabs((q * q - 1.) / (q * q + 1.));
+    }
+    case LT_MAP_SHEAR3:
+    case LT_MAP_GAMMA1: return (a - c) * D / 2.;
+    case LT_MAP_SHEAR4:
+    case LT_MAP_GAMMA2: return b * D;
+    case LT_MAP_KAPPA: return (a + c) * D / 2.;
+    case LT_MAP_MU: {
+        double k = (a + c) * D / 2.;
+        double g1 = (a - c) * D / 2.;
+        double g2 = b * D;
+        return 1. / ((1. - k) * (1. - k) - g1 * g1 - g2 * g2);
+    }
+    case LT_MAP_MASS: return (a + c) * 0.5 * mult;
+    case KIND_GRAD_X: return gx * scale;
+    case KIND_GRAD_Y: return gy * scale;
+    case KIND_POT: return psi * scale;
+    default: return 0.;
+    }
+}
+
+} // namespace lt

@@ -1,0 +1,521 @@
+/*
+ * lt_capi.cpp -- the extern "C" entry points of include/lt_b200.h: contexts, catalogue
+ * validation/packing/upload, and the grid calls (argument checks, host staging, launch).
+ */
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lt_b200.h"
+#include "lt_grid.cuh"
+#include "lt_halo.h"
+#include "lt_internal.h"
+
+using namespace lt;
+
+static std::atomic<uint64_t> g_launches{0};
+
+namespace lt {
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+} // namespace lt
+
+struct lt_catalog {
+    lt_rec64 *recs = nullptr;
+    lt_chunk *chunks = nullptr;
+    int32_t nhalos = 0;
+    int32_t nchunks = 0;
+    size_t bytes = 0;
+    std::vector<lt_rec64> host_recs; /* packed copy, reused by the FP32 packing */
+    void *aux = nullptr;             /* precision-specific device data */
+    size_t aux_bytes = 0;
+};
+
+/* ------------------------------------------------------------------ helpers ---- */
+
+void lt::set_error(lt_context *ctx, const char *fmt, ...)
+{
+    if (!ctx) return;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+}
+
+lt_status lt::cuda_fail(lt_context *ctx, cudaError_t e, const char *what)
+{
+    set_error(ctx, "%s: %s", what, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return LT_ERR_OUT_OF_MEMORY;
+    return LT_ERR_CUDA;
+}
+
+lt_status lt::dev_alloc(lt_context *ctx, void **p, size_t bytes)
+{
+    if (ctx->used + bytes > ctx->budget) {
+        set_error(ctx, "HBM budget exceeded: %zu in use + %zu requested > %zu", ctx->used, bytes, ctx->budget);
+        return LT_ERR_BUDGET;
+    }
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaMalloc");
+    ctx->used += bytes;
+    return LT_OK;
+}
+
+void lt::dev_free(lt_context *ctx, void *p, size_t bytes)
+{
+    if (!p) return;
+    cudaFree(p);
+    ctx->used -= bytes;
+}
+
+/* Device staging planes for host-pointer outputs, grown on demand. */
+lt_status lt::scratch_planes(lt_context *ctx, int n, size_t plane_bytes, double **planes)
+{
+    size_t need = (size_t)n * plane_bytes;
+    if (need > ctx->scratch_bytes) {
+        dev_free(ctx, ctx->scratch, ctx->scratch_bytes);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+        lt_status st = dev_alloc(ctx, &ctx->scratch, need);
+        if (st != LT_OK) return st;
+        ctx->scratch_bytes = need;
+    }
+    for (int i = 0; i < n; i++) planes[i] = (double *)((char *)ctx->scratch + (size_t)i * plane_bytes);
+    return LT_OK;
+}
+
+bool lt::is_device_pointer(const void *p)
+{
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+/* ---------------------------------------------------------------- packing ---- */
+
+/* Per-halo invariants (see lt_halo.h for the slot meaning).  The expressions are the
+ * reference's own sub-expressions: src/gradient.cpp:764-783 (cut dPIE deflection),
+ * src/gradient2.cpp:57-66 (mdci05), src/potential_GPU.cu:52-58 (pi05). */
+static void pack_one(const lt_halo_soa *s, int i, lt_rec64 &r)
+{
+    const int t = s->type[i];
+    const double e = s->ellipticity_potential[i];
+    const double rc = s->rcore[i], rcut = s->rcut[i], b0 = s->b0[i];
+    memset(&r, 0, sizeof(r));
+    r.x0 = s->position_x[i];
+    r.y0 = s->position_y[i];
+    r.cs = s->anglecos[i];
+    r.sn = s->anglesin[i];
+    r.b0 = b0;
+    r.eps = e;
+    r.rc = rc;
+    r.rcut = rcut;
+    r.w = s->dlsds ? s->dlsds[i] : 1.0;
+    if (t == 5) {
+        r.cx1 = 1. - e;
+        r.cx1inv = 1. + e;
+        r.pref_g = (1. - e) * b0;
+        r.pref_h = (1. + e) * b0;
+        r.ci = b0 * (1. - e) * (1. + e);
+        return;
+    }
+    const double sqe = sqrt(e);
+    r.sqe2 = 2. * sqe;
+    r.cx1 = (1. - e) / (1. + e);
+    r.cx1inv = 1. / r.cx1;
+    r.cxro_inv = 1. / ((1. + e) * (1. + e));
+    r.cyro_inv = 1. / ((1. - e) * (1. - e));
+    r.k4 = 4. * e;
+    r.ci = 0.5 * (1. - e * e) / sqe;
+    const double t05 = (t == 81) ? rcut / (rcut - rc) : 1.0;
+    r.pref_g = r.ci * b0 * t05;
+    r.pref_h = r.ci * b0 * t05;
+    r.rc2 = rc * rc;
+    r.rcut2 = rcut * rcut;
+    r.tsr_c = 2. * rc * sqe;
+    r.tsr_t = 2. * rcut * sqe;
+    r.e1 = 2. * sqe / (1 - e);
+    r.e2 = 2. * sqe / (1 + e);
+}
+
+/* Domain checks: the reference would divide by zero or take sqrt of a negative value
+ * (and silently produce NaN maps); here the upload fails with a status instead. */
+static lt_status validate(lt_context *ctx, const lt_halo_soa *s)
+{
+    for (int i = 0; i < s->nhalos; i++) {
+        const int t = s->type[i];
+        if (t != 5 && t != 8 && t != 81) {
+            set_error(ctx, "halo %d: unknown profile type %d (supported: 5, 8, 81)", i, t);
+            return LT_ERR_UNKNOWN_PROFILE;
+        }
+        const double v[] = {s->position_x[i], s->position_y[i], s->b0[i], s->anglecos[i], s->anglesin[i],
+                            s->ellipticity_potential[i], s->rcore[i], s->rcut[i], s->dlsds ? s->dlsds[i] : 1.0};
+        for (double x : v)
+            if (!std::isfinite(x)) {
+                set_error(ctx, "halo %d: non-finite parameter", i);
+                return LT_ERR_NONFINITE;
+            }
+        const double e = s->ellipticity_potential[i];
+        if (t == 5 ? !(e >= 0. && e < 1.) : !(e > 0. && e < 1.)) {
+            set_error(ctx, "halo %d: ellipticity_potential %g outside the profile's domain", i, e);
+            return LT_ERR_NONFINITE;
+        }
+        if (t != 5 && !(s->rcore[i] > 0.)) {
+            set_error(ctx, "halo %d: rcore must be > 0", i);
+            return LT_ERR_NONFINITE;
+        }
+        if (t == 81 && !(s->rcut[i] > s->rcore[i])) {
+            set_error(ctx, "halo %d: rcut must exceed rcore for the cut dPIE", i);
+            return LT_ERR_NONFINITE;
+        }
+    }
+    return LT_OK;
+}
+
+std::vector<lt_chunk> lt::make_chunks(const int32_t *type, int n, int max_chunk)
+{
+    std::vector<lt_chunk> ch;
+    int s = 0;
+    while (s < n) {
+        int e = s + 1;
+        while (e < n && type[e] == type[s]) e++;
+        for (int c = s; c < e; c += max_chunk) {
+            lt_chunk k;
+            k.start = c;
+            k.count = (e - c) < max_chunk ? (e - c) : max_chunk;
+            k.type = type[s];
+            k.pad = 0;
+            ch.push_back(k);
+        }
+        s = e;
+    }
+    return ch;
+}
+
+/* ------------------------------------------------------------------- API ---- */
+
+extern "C" {
+
+int32_t lt_abi_version(void) { return LT_B200_ABI_VERSION; }
+
+uint64_t lt_kernel_launch_count(void) { return g_launches.load(); }
+
+const char *lt_status_string(lt_status s)
+{
+    switch (s) {
+    case LT_OK: return "ok";
+    case LT_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case LT_ERR_UNKNOWN_PROFILE: return "unknown profile type";
+    case LT_ERR_NONFINITE: return "non-finite or out-of-domain halo parameter";
+    case LT_ERR_CUDA: return "CUDA error";
+    case LT_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case LT_ERR_BUDGET: return "HBM budget exceeded";
+    case LT_ERR_QUEUE_FULL: return "queue full";
+    case LT_ERR_TIMEOUT: return "device-side wait timed out";
+    case LT_ERR_NO_DEVICE: return "no usable CUDA device";
+    case LT_ERR_NOT_READY: return "not ready";
+    }
+    return "unknown status";
+}
+
+const char *lt_last_error(const lt_context *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+lt_status lt_create(int device, size_t budget, lt_context **out)
+{
+    if (!out) return LT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return LT_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return LT_ERR_NO_DEVICE;
+    if (prop.major < 10) return LT_ERR_NO_DEVICE; /* built for sm_100a only */
+    lt_context *ctx = new (std::nothrow) lt_context();
+    if (!ctx) return LT_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    cudaSetDevice(device);
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    ctx->budget = budget ? budget : (size_t)(0.9 * (double)free_b);
+    ctx->used = 0;
+    lt_status st = dev_alloc(ctx, (void **)&ctx->status, 64);
+    if (st != LT_OK) {
+        delete ctx;
+        return st;
+    }
+    cudaMemset(ctx->status, 0, 64);
+    *out = ctx;
+    return LT_OK;
+}
+
+lt_status lt_destroy(lt_context *ctx)
+{
+    if (!ctx) return LT_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    dev_free(ctx, ctx->scratch, ctx->scratch_bytes);
+    dev_free(ctx, ctx->status, 64);
+    destroy_extensions(ctx);
+    delete ctx;
+    return LT_OK;
+}
+
+lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *s, lt_catalog **out)
+{
+    if (!ctx || !s || !out || s->nhalos < 0) return LT_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (s->nhalos > 0 && (!s->type || !s->position_x || !s->position_y || !s->b0 || !s->anglecos ||
+                          !s->anglesin || !s->ellipticity_potential || !s->rcore || !s->rcut)) {
+        set_error(ctx, "catalogue field pointer is NULL");
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    lt_status st = validate(ctx, s);
+    if (st != LT_OK) return st;
+    lt_catalog *cat = new (std::nothrow) lt_catalog();
+    if (!cat) return LT_ERR_OUT_OF_MEMORY;
+    cat->nhalos = s->nhalos;
+    cat->host_recs.resize(s->nhalos);
+    for (int i = 0; i < s->nhalos; i++) pack_one(s, i, cat->host_recs[i]);
+    std::vector<lt_chunk> ch = make_chunks(s->type, s->nhalos, LT_CHUNK);
+    cat->nchunks = (int32_t)ch.size();
+    size_t rb = sizeof(lt_rec64) * (size_t)s->nhalos, cb = sizeof(lt_chunk) * ch.size();
+    cat->bytes = rb + cb;
+    st = dev_alloc(ctx, (void **)&cat->recs, rb);
+    if (st == LT_OK) st = dev_alloc(ctx, (void **)&cat->chunks, cb);
+    if (st == LT_OK && rb) {
+        cudaError_t e = cudaMemcpy(cat->recs, cat->host_recs.data(), rb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && cb) e = cudaMemcpy(cat->chunks, ch.data(), cb, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, "catalogue upload");
+    }
+    if (st == LT_OK) st = prepare_catalog_extensions(ctx, cat);
+    if (st != LT_OK) {
+        lt_catalog_release(ctx, cat);
+        return st;
+    }
+    *out = cat;
+    return LT_OK;
+}
+
+lt_status lt_catalog_release(lt_context *ctx, lt_catalog *cat)
+{
+    if (!ctx || !cat) return LT_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    dev_free(ctx, cat->recs, sizeof(lt_rec64) * (size_t)cat->nhalos);
+    dev_free(ctx, cat->chunks, sizeof(lt_chunk) * (size_t)cat->nchunks);
+    dev_free(ctx, cat->aux, cat->aux_bytes);
+    delete cat;
+    return LT_OK;
+}
+
+int32_t lt_catalog_nhalos(const lt_catalog *cat) { return cat ? cat->nhalos : -1; }
+
+lt_status lt_synchronize(lt_context *ctx, void *stream)
+{
+    if (!ctx) return LT_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "stream synchronize");
+    int32_t st = 0;
+    e = cudaMemcpy(&st, ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "status read");
+    if (st != 0) {
+        cudaMemset(ctx->status, 0, sizeof(int32_t));
+        set_error(ctx, "kernel reported status %d", st);
+        return (lt_status)st;
+    }
+    return LT_OK;
+}
+
+} // extern "C"
+
+/* ------------------------------------------------------------- grid calls ---- */
+
+static bool grid_ok(const lt_grid *g)
+{
+    return g && g->nx > 0 && g->ny > 0 && std::isfinite(g->xmin) && std::isfinite(g->ymin) &&
+           std::isfinite(g->dx) && std::isfinite(g->dy) && (long)g->nx * g->ny <= (1L << 31);
+}
+
+/* Run one grid evaluation: `kinds`/`outs` are the requested planes (host or device). */
+lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g, int precision, int op, int kmap,
+                       double D, double mult, double scale, int nout, const int *kinds, double *const *outs,
+                       void *stream)
+{
+    if (!ctx || !cat || !grid_ok(g) || nout < 1 || nout > LT_MAX_MAPS) {
+        if (ctx) set_error(ctx, "invalid grid-call arguments");
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    if (precision != LT_FP64 && precision != LT_FP32C) {
+        set_error(ctx, "unknown precision %d", precision);
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    for (int i = 0; i < nout; i++)
+        if (!outs[i]) {
+            set_error(ctx, "output %d is NULL", i);
+            return LT_ERR_INVALID_ARGUMENT;
+        }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    const size_t npix = (size_t)g->nx * g->ny;
+    const size_t plane = npix * sizeof(double);
+    bool host = false;
+    for (int i = 0; i < nout; i++) host |= !is_device_pointer(outs[i]);
+    double *dev_out[LT_MAX_MAPS];
+    if (host) {
+        lt_status st = scratch_planes(ctx, nout, plane, dev_out);
+        if (st != LT_OK) return st;
+    } else {
+        for (int i = 0; i < nout; i++) dev_out[i] = outs[i];
+    }
+    GridArgs a;
+    memset(&a, 0, sizeof(a));
+    a.recs = cat->recs;
+    a.chunks = cat->chunks;
+    a.nchunks = cat->nchunks;
+    a.kmap = kmap;
+    a.xmin = g->xmin;
+    a.ymin = g->ymin;
+    a.dx = g->dx;
+    a.dy = g->dy;
+    a.nx = g->nx;
+    a.ny = g->ny;
+    a.istart = g->istart;
+    a.jstart = g->jstart;
+    a.nout = nout;
+    a.vec_ok = (g->nx % 2 == 0);
+    for (int i = 0; i < nout; i++) {
+        a.kinds[i] = kinds[i];
+        a.out[i] = dev_out[i];
+        if (((uintptr_t)dev_out[i]) % 16) a.vec_ok = 0;
+    }
+    a.D = D;
+    a.mult = mult;
+    a.scale = scale;
+    a.status = ctx->status;
+    cudaStream_t s = (cudaStream_t)stream;
+    int err;
+    if (cat->nhalos == 0) {
+        for (int i = 0; i < nout; i++) cudaMemsetAsync(dev_out[i], 0, plane, s);
+        err = cudaSuccess;
+        if (kinds[0] != KIND_GRAD_X) {
+            /* maps of an empty catalogue: evaluate the epilogue on zero sums */
+            err = launch_epilogue_zero(a, ctx->num_sms, s);
+            count_launch(1);
+        }
+    } else if (precision == LT_FP64) {
+        err = launch_grid64_tiled(op, a, ctx->num_sms, s);
+    } else {
+        err = launch_fp32c(ctx, cat, op, a, s);
+    }
+    if (err != cudaSuccess) return cuda_fail(ctx, (cudaError_t)err, "grid kernel launch");
+    if (host) {
+        for (int i = 0; i < nout; i++) {
+            cudaError_t e = cudaMemcpyAsync(outs[i], dev_out[i], plane, cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+        }
+        return lt_synchronize(ctx, stream);
+    }
+    return LT_OK;
+}
+
+/* Tile bookkeeping shared by the launchers. */
+int lt::launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream)
+{
+    const int tile_w = 64, tile_h = 8;
+    a.tiles_x = (a.nx + tile_w - 1) / tile_w;
+    a.ntiles = a.tiles_x * ((a.ny + tile_h - 1) / tile_h);
+    int err = launch_grid64(op, a, num_sms, stream);
+    count_launch(1);
+    return err;
+}
+
+extern "C" {
+
+lt_status lt_gradient_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                           double scale, double *ax, double *ay, void *stream)
+{
+    const int kinds[2] = {KIND_GRAD_X, KIND_GRAD_Y};
+    double *outs[2] = {ax, ay};
+    return run_grid(ctx, cat, grid, precision, OP_GRAD, 0, 1.0, 1.0, scale, 2, kinds, outs, stream);
+}
+
+static bool hess_kind_ok(int k)
+{
+    return (k >= LT_MAP_HESS_A && k <= LT_MAP_HESS_D) || (k >= LT_MAP_AMPLI1 && k <= LT_MAP_AMPLI6) ||
+           (k >= LT_MAP_SHEAR1 && k <= LT_MAP_SHEAR4) || (k >= LT_MAP_KAPPA && k <= LT_MAP_MU) || k == LT_MAP_MASS;
+}
+
+lt_status lt_hessian_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                          int32_t kmap, double dlsds, double mult, const lt_map_request *maps, int32_t nmaps,
+                          void *stream)
+{
+    if (!maps || nmaps < 1 || nmaps > LT_MAX_MAPS) {
+        if (ctx) set_error(ctx, "between 1 and %d maps must be requested", LT_MAX_MAPS);
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    int kinds[LT_MAX_MAPS];
+    double *outs[LT_MAX_MAPS];
+    for (int i = 0; i < nmaps; i++) {
+        if (!hess_kind_ok(maps[i].kind)) {
+            if (ctx) set_error(ctx, "unknown map kind %d", maps[i].kind);
+            return LT_ERR_INVALID_ARGUMENT;
+        }
+        kinds[i] = maps[i].kind;
+        outs[i] = maps[i].out;
+    }
+    return run_grid(ctx, cat, grid, precision, OP_HESS, kmap ? 1 : 0, dlsds, mult, 1.0, nmaps, kinds, outs, stream);
+}
+
+lt_status lt_potential_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
+                            double scale, double *psi, void *stream)
+{
+    const int kinds[1] = {KIND_POT};
+    double *outs[1] = {psi};
+    return run_grid(ctx, cat, grid, precision, OP_POT, 0, 1.0, 1.0, scale, 1, kinds, outs, stream);
+}
+
+lt_status lt_lens_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision, double dlsds,
+                       double *kappa, double *gamma1, double *gamma2, double *mu, double *psi, void *stream)
+{
+    int kinds[5];
+    double *outs[5];
+    int n = 0, op = 0;
+    const int ks[4] = {LT_MAP_KAPPA, LT_MAP_GAMMA1, LT_MAP_GAMMA2, LT_MAP_MU};
+    double *os[4] = {kappa, gamma1, gamma2, mu};
+    for (int i = 0; i < 4; i++)
+        if (os[i]) {
+            kinds[n] = ks[i];
+            outs[n++] = os[i];
+            op |= OP_HESS;
+        }
+    if (psi) {
+        kinds[n] = KIND_POT;
+        outs[n++] = psi;
+        op |= OP_POT;
+    }
+    if (n == 0) {
+        if (ctx) set_error(ctx, "no output requested");
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    return run_grid(ctx, cat, grid, precision, op, 0, dlsds, 1.0, dlsds, n, kinds, outs, stream);
+}
+
+} // extern "C"

@@ -1,0 +1,39 @@
+/*
+ * lt_grid.cuh -- launch arguments shared by the grid kernels and the host launchers.
+ */
+#pragma once
+#include <stdint.h>
+#include "lt_halo.h"
+#include "../../include/lt_b200.h"
+
+namespace lt {
+
+/* internal output kinds besides lt_map_kind */
+enum {
+    KIND_GRAD_X = 100, /* deflection x * scale */
+    KIND_GRAD_Y = 101, /* deflection y * scale */
+    KIND_POT = 102     /* potential * scale */
+};
+
+/* which sums a kernel evaluates */
+enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4 };
+
+struct GridArgs {
+    const lt_rec64 *recs;
+    const lt_chunk *chunks;
+    int32_t nchunks;
+    int32_t kmap;
+    double xmin, ymin, dx, dy;
+    int32_t nx, ny, istart, jstart;
+    int32_t tiles_x, ntiles;
+    int32_t nout, vec_ok;
+    int32_t kinds[LT_MAX_MAPS];
+    double *out[LT_MAX_MAPS];
+    double D, mult, scale;
+    int32_t *status; /* device word: 0, or an lt_status set by a kernel */
+};
+
+/* Launch the FP64 grid kernel for the sums in `op` (OP_* mask).  Returns the CUDA error. */
+int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream);
+
+} // namespace lt

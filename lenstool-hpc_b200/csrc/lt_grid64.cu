@@ -1,0 +1,202 @@
+/*
+ * lt_grid64.cu -- FP64 persistent grid kernel: deflection, Hessian (+ map epilogue) and
+ * potential sums over a packed halo catalogue.
+ *
+ * Work layout
+ *   - A CTA of 256 threads owns a pixel tile of (32 P) x 8 pixels; each thread owns P
+ *     adjacent pixels of one row (P = 2: one 16-byte store per output plane).
+ *   - CTAs are persistent: grid = resident CTAs per SM x SMs, tiles strided by gridDim.
+ *   - The halo catalogue is walked in chunks of LT_CHUNK records (each chunk holds one
+ *     profile type).  Chunk k+1 is brought into shared memory by one cp.async.bulk
+ *     while chunk k is evaluated; every thread then reads the same record (a shared-memory
+ *     broadcast), so the per-halo invariants cost no global traffic in the pair loop.
+ *   - The pair loop is specialised per profile type (no function pointers, unlike the
+ *     reference's device function tables, src/gradient_GPU.cu:910-922).
+ */
+#include <cuda_runtime.h>
+#include "lt_bulk.cuh"
+#include "lt_profiles64.cuh"
+
+namespace lt {
+
+constexpr int kThreads = 256;
+
+template <int OP, int P>
+struct Acc64 {
+    double gx[P], gy[P], hxx[P], hyy[P], hxy[P], psi[P];
+};
+
+template <int OP, int P, int TYPE>
+__device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, const double (&px)[P], double py,
+                                             int kmap, Acc64<OP, P> &acc)
+{
+#pragma unroll 1
+    for (int h = 0; h < count; h++) {
+        const lt_rec64 &r = recs[h];
+        double w = kmap ? r.w : 1.0;
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            if (OP & OP_GRAD) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
+            if (OP & OP_HESS) {
+                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
+                hess_pair<TYPE>(r, px[k], py, w, hh);
+                acc.hxx[k] = hh.xx;
+                acc.hyy[k] = hh.yy;
+                acc.hxy[k] = hh.xy;
+            }
+            if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
+        }
+    }
+}
+
+template <int OP, int P>
+__global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    lt_rec64 *buf0 = reinterpret_cast<lt_rec64 *>(smem);
+    lt_rec64 *buf1 = buf0 + LT_CHUNK;
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int kTileW = 32 * P;
+    const int ox = (warp & 3) * (8 * P) + (lane & 7) * P; /* pixel offset in the tile */
+    const int oy = (warp >> 2) * 4 + (lane >> 3);
+
+    const int my_tiles = (blockIdx.x < a.ntiles) ? (a.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const long steps = (long)my_tiles * a.nchunks;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (steps == 0) return;
+
+    auto issue = [&](long s) {
+        const lt_chunk c = a.chunks[s % a.nchunks];
+        lt_rec64 *dst = (s & 1) ? buf1 : buf0;
+        uint64_t *bar = &bars[s & 1];
+        uint32_t bytes = (uint32_t)c.count * (uint32_t)sizeof(lt_rec64);
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_g2s(dst, a.recs + c.start, bytes, bar);
+    };
+    if (tid == 0) issue(0);
+
+    uint32_t phase0 = 0, phase1 = 0;
+    Acc64<OP, P> acc;
+    double px[P], py = 0.;
+    int ix = 0, iy = 0;
+
+    for (long s = 0; s < steps; s++) {
+        const int ci = (int)(s % a.nchunks);
+        if (ci == 0) {
+            const int tile = blockIdx.x + (int)(s / a.nchunks) * gridDim.x;
+            const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+            ix = tx * kTileW + ox;
+            iy = ty * 8 + oy;
+            const int cy = iy < a.ny ? iy : a.ny - 1;
+            py = pixel_y(a, cy);
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                const int cx = (ix + k) < a.nx ? ix + k : a.nx - 1;
+                px[k] = pixel_x(a, cx);
+                acc.gx[k] = acc.gy[k] = acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
+            }
+        }
+        if (tid == 0 && s + 1 < steps) issue(s + 1);
+
+        const int b = (int)(s & 1);
+        uint64_t *bar = &bars[b];
+        const uint32_t par = b ? phase1 : phase0;
+        if (!wait_tile(bar, par, a.status)) {
+            if (tid == 0 && s + 1 < steps) drain_tile(&bars[b ^ 1], b ? phase0 : phase1);
+            return;
+        }
+        if (b) phase1 ^= 1; else phase0 ^= 1;
+
+        const lt_chunk c = a.chunks[ci];
+        const lt_rec64 *recs = b ? buf1 : buf0;
+        switch (c.type) {
+        case 81: eval_chunk64<OP, P, 81>(recs, c.count, px, py, a.kmap, acc); break;
+        case 8: eval_chunk64<OP, P, 8>(recs, c.count, px, py, a.kmap, acc); break;
+        case 5: eval_chunk64<OP, P, 5>(recs, c.count, px, py, a.kmap, acc); break;
+        default: break;
+        }
+
+        if (ci == a.nchunks - 1 && iy < a.ny) {
+            const long row = (long)iy * a.nx;
+            const bool full = a.vec_ok && (ix + P <= a.nx);
+            for (int o = 0; o < a.nout; o++) {
+                double v[P];
+#pragma unroll
+                for (int k = 0; k < P; k++)
+                    v[k] = map_value(a.kinds[o], acc.gx[k], acc.gy[k], acc.hxx[k], acc.hyy[k], acc.hxy[k], acc.psi[k],
+                                     a.D, a.mult, a.scale);
+                double *dst = a.out[o] + row + ix;
+                if (P == 2 && full) {
+                    *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1 % P]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < P; k++)
+                        if (ix + k < a.nx) dst[k] = v[k];
+                }
+            }
+        }
+        __syncthreads(); /* buffer b is refilled by the copy issued at step s + 1 */
+    }
+}
+
+template <int OP, int P>
+static int launch_op(const GridArgs &args, int num_sms, cudaStream_t stream)
+{
+    const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
+    auto kern = grid64_kernel<OP, P>;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = true;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    int blocks = num_sms * per_sm;
+    if (blocks > args.ntiles) blocks = args.ntiles;
+    if (blocks < 1) blocks = 1;
+    kern<<<blocks, kThreads, smem, stream>>>(args);
+    return (int)cudaGetLastError();
+}
+
+int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (op) {
+    case OP_GRAD: return launch_op<OP_GRAD, 2>(args, num_sms, s);
+    case OP_HESS: return launch_op<OP_HESS, 2>(args, num_sms, s);
+    case OP_POT: return launch_op<OP_POT, 2>(args, num_sms, s);
+    case OP_HESS | OP_POT: return launch_op<OP_HESS | OP_POT, 2>(args, num_sms, s);
+    default: return (int)cudaErrorInvalidValue;
+    }
+}
+
+} // namespace lt
+
+namespace lt {
+
+/* Maps of an empty catalogue: the epilogue evaluated on zero sums. */
+__global__ void epilogue_zero_kernel(const GridArgs a)
+{
+    const long npix = (long)a.nx * a.ny;
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x)
+        for (int o = 0; o < a.nout; o++) a.out[o][p] = map_value(a.kinds[o], 0., 0., 0., 0., 0., 0., a.D, a.mult, a.scale);
+}
+
+int launch_epilogue_zero(const GridArgs &a, int num_sms, void *stream)
+{
+    epilogue_zero_kernel<<<num_sms * 4, 256, 0, (cudaStream_t)stream>>>(a);
+    return (int)cudaGetLastError();
+}
+
+} // namespace lt

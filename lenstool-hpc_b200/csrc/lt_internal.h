@@ -1,0 +1,48 @@
+/*
+ * lt_internal.h -- library-internal declarations shared by the C-ABI translation units.
+ */
+#pragma once
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lt_b200.h"
+#include "lt_grid.cuh"
+#include "lt_halo.h"
+
+struct lt_context {
+    int device = 0;
+    int num_sms = 0;
+    size_t budget = 0, used = 0;
+    std::mutex mu;
+    std::string last_error;
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    int32_t *status = nullptr; /* device status word written by kernels */
+    void *ext = nullptr;       /* state of the batch and serving extensions */
+};
+
+namespace lt {
+
+void count_launch(uint64_t n);
+void set_error(lt_context *ctx, const char *fmt, ...);
+lt_status cuda_fail(lt_context *ctx, cudaError_t e, const char *what);
+lt_status dev_alloc(lt_context *ctx, void **p, size_t bytes);
+void dev_free(lt_context *ctx, void *p, size_t bytes);
+lt_status scratch_planes(lt_context *ctx, int n, size_t plane_bytes, double **planes);
+bool is_device_pointer(const void *p);
+std::vector<lt_chunk> make_chunks(const int32_t *type, int n, int max_chunk);
+
+lt_status run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g, int precision, int op, int kmap, double D,
+                   double mult, double scale, int nout, const int *kinds, double *const *outs, void *stream);
+int launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream);
+int launch_epilogue_zero(const GridArgs &a, int num_sms, void *stream);
+
+/* FP32-compensated path (lt_grid32.cu) */
+lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat);
+int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, void *stream);
+void destroy_extensions(lt_context *ctx);
+
+} // namespace lt

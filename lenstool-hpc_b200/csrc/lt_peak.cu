@@ -1,0 +1,68 @@
+/*
+ * lt_peak.cu -- FMA-pipe throughput of the current GPU, measured with independent FMA
+ * chains.  The grid kernels here are bound by the FP64 or FP32 pipe rather than by HBM
+ * or the tensor cores; this number is the denominator of their roofline fraction.
+ */
+#include <cuda_runtime.h>
+
+#include "lt_internal.h"
+
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kIters = 4096;
+
+template <typename T>
+__global__ void fma_chain_kernel(T seed, T *sink)
+{
+    T a = seed + (T)threadIdx.x * (T)1e-7, b = (T)0.999999;
+    T acc[kChains];
+#pragma unroll
+    for (int c = 0; c < kChains; c++) acc[c] = a + (T)c;
+#pragma unroll 4
+    for (int i = 0; i < kIters; i++) {
+#pragma unroll
+        for (int c = 0; c < kChains; c++) acc[c] = fma(acc[c], b, a);
+    }
+    T s = 0;
+#pragma unroll
+    for (int c = 0; c < kChains; c++) s += acc[c];
+    if (s == (T)-12345.) sink[0] = s; /* keeps the chains live; never true */
+}
+
+template <typename T>
+double measure(int device)
+{
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return 0.;
+    cudaSetDevice(device);
+    T *sink = nullptr;
+    if (cudaMalloc(&sink, sizeof(T)) != cudaSuccess) return 0.;
+    const int threads = 256, blocks = prop.multiProcessorCount * 8;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0.;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0);
+        fma_chain_kernel<T><<<blocks, threads>>>((T)1.0, sink);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        double flops = 2.0 * kChains * (double)kIters * threads * blocks;
+        if (rep > 0 && ms > 0.f) best = flops / (ms * 1e-3) / 1e12 > best ? flops / (ms * 1e-3) / 1e12 : best;
+    }
+    lt::count_launch(4);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    return best;
+}
+
+} // namespace
+
+extern "C" double lt_measure_fma_peak(int fp32, int device)
+{
+    return fp32 ? measure<float>(device) : measure<double>(device);
+}

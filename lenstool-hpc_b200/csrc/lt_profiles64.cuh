@@ -1,0 +1,221 @@
+/*
+ * lt_profiles64.cuh -- FP64 per-pair profile arithmetic (one halo record, one pixel).
+ *
+ * Formulas follow the reference's FP64 CPU path; divisions by per-halo constants
+ * become multiplications by the precomputed reciprocals of lt_rec64, and divisions by
+ * per-pair denominators are done once as a reciprocal.  These changes move results by
+ * a few ulp; the tests hold this path to 1e-12 of the reference.
+ *
+ *   deflection:  SIS src/gradient.cpp:260-299, PIEMD :548-607, dPIE :744-811,
+ *                complex-log term KERNEL src/gradient.hpp:64-76
+ *   Hessian:     dPIE src/gradient2.cpp:92-205 with mdci05 :54-83; PIEMD = one mdci05
+ *                term; SIS = derivative of the SIS deflection (restated)
+ *   potential:   dPIE src/potential_GPU.cu:47-116 (pi05 with the complex helpers of
+ *                src/lt_math_GPU.cuh); PIEMD = one pi05 term; SIS = b0 R (restated)
+ */
+#pragma once
+#include "lt_halo.h"
+
+namespace lt {
+
+struct Frame64 {
+    double u, v;
+};
+
+/* Offset from the halo centre rotated into the halo frame (x' = x cos + y sin,
+ * y' = y cos - x sin; src/gradient.hpp:29-37). */
+__device__ __forceinline__ Frame64 to_frame(const lt_rec64 &h, double px, double py)
+{
+    double tx = px - h.x0, ty = py - h.y0;
+    Frame64 f;
+    f.u = tx * h.cs + ty * h.sn;
+    f.v = ty * h.cs - tx * h.sn;
+    return f;
+}
+
+/* ---------------------------------------------------------------- deflection ---- */
+
+/* log|z|^2 and arg z of the PIEMD complex ratio for one radius (KERNEL macro). */
+__device__ __forceinline__ void piemd_log_term(double u, double uu, double v, double nre, double vq, double sqe2,
+                                               double rem2, double r2, double tsr, double &lq, double &la)
+{
+    double nim = sqe2 * sqrt(r2 + rem2) - vq;
+    double dim = tsr - v;
+    double inv = 1.0 / (uu + dim * dim);
+    double zre = (nre * u + nim * dim) * inv;
+    double zim = (nim * u - nre * dim) * inv;
+    lq = log(zre * zre + zim * zim);
+    la = atan2(zim, zre);
+}
+
+template <int TYPE>
+__device__ __forceinline__ void grad_pair(const lt_rec64 &h, double px, double py, double &gx, double &gy)
+{
+    Frame64 f = to_frame(h, px, py);
+    double u = f.u, v = f.v;
+    if (TYPE == 5) {
+        /* inverse radius from a single-precision root and one Newton step, as the
+         * reference (src/gradient.cpp:287-288) */
+        double q = u * u * h.cx1 + v * v * h.cx1inv;
+        double r = 1. / (double)sqrtf((float)q);
+        r = r * (1.5 - 0.5 * q * r * r);
+        double fx = h.pref_g * u * r;
+        double fy = h.pref_h * v * r;
+        gx += fx * h.cs - fy * h.sn;
+        gy += fy * h.cs + fx * h.sn;
+    } else {
+        double uu = u * u;
+        double rem2 = uu * h.cxro_inv + v * v * h.cyro_inv;
+        double vq = v * h.cx1inv;
+        double nre = h.cx1 * u;
+        double lq, la;
+        piemd_log_term(u, uu, v, nre, vq, h.sqe2, rem2, h.rc2, h.tsr_c, lq, la);
+        double re, im;
+        if (TYPE == 81) {
+            double lq2, la2;
+            piemd_log_term(u, uu, v, nre, vq, h.sqe2, rem2, h.rcut2, h.tsr_t, lq2, la2);
+            re = h.pref_g * (la - la2);
+            im = -0.5 * h.pref_g * (lq - lq2);
+        } else {
+            re = h.pref_g * la;
+            im = -0.5 * h.pref_g * lq;
+        }
+        gx += re * h.cs - im * h.sn;
+        gy += im * h.cs + re * h.sn;
+    }
+}
+
+/* ------------------------------------------------------------------- Hessian ---- */
+
+struct Hess64 {
+    double xx, yy, xy;
+};
+
+/* The three bracketed terms of mdci05 (didxre, didyre, didyim without the factor ci). */
+__device__ __forceinline__ void mdci05_terms(const lt_rec64 &h, double u, double uu, double v, double vv,
+                                             double vq, double rem2, double r2, double tsr, double &X, double &Y,
+                                             double &Z)
+{
+    double wrem = sqrt(r2 + rem2);
+    double iw = 1.0 / wrem;
+    double t1 = h.sqe2 * wrem - vq;
+    double den1 = h.cx1 * h.cx1 * uu + t1 * t1;
+    double num2 = tsr - v;
+    double den2 = uu + num2 * num2;
+    double i1 = 1.0 / den1;
+    double i2 = 1.0 / den2;
+    X = h.cx1 * (h.sqe2 * uu * h.cxro_inv * iw - h.sqe2 * wrem + vq) * i1 + num2 * i2;
+    Y = (h.sqe2 * u * v * h.cx1 * h.cyro_inv * iw - u) * i1 + u * i2;
+    Z = (h.sqe2 * wrem * h.cx1inv - vq * h.cx1inv - h.k4 * v * h.cyro_inv + h.sqe2 * vv * h.cyro_inv * iw * h.cx1inv) * i1 -
+        num2 * i2;
+}
+
+/* H = R^T H' R for the symmetric halo-frame Hessian H' = [[a, b], [b, c]]; the
+ * reference applies the same rotation in two steps (src/gradient2.cpp:146-156). */
+__device__ __forceinline__ void rotate_acc(const lt_rec64 &h, double a, double b, double c, double w, Hess64 &acc)
+{
+    double cs = h.cs, sn = h.sn;
+    double cc = cs * cs, ss = sn * sn, csn = cs * sn;
+    acc.xx += w * (a * cc - 2. * b * csn + c * ss);
+    acc.yy += w * (a * ss + 2. * b * csn + c * cc);
+    acc.xy += w * ((a - c) * csn + b * (cc - ss));
+}
+
+template <int TYPE>
+__device__ __forceinline__ void hess_pair(const lt_rec64 &h, double px, double py, double w, Hess64 &acc)
+{
+    Frame64 f = to_frame(h, px, py);
+    double u = f.u, v = f.v;
+    double uu = u * u, vv = v * v;
+    if (TYPE == 5) {
+        double q = uu * h.cx1 + vv * h.cx1inv;
+        double r = sqrt(q);
+        double k = h.ci / (q * r);
+        rotate_acc(h, k * vv, -k * u * v, k * uu, w, acc);
+    } else {
+        double rem2 = uu * h.cxro_inv + vv * h.cyro_inv;
+        double vq = v * h.cx1inv;
+        double X, Y, Z;
+        mdci05_terms(h, u, uu, v, vv, vq, rem2, h.rc2, h.tsr_c, X, Y, Z);
+        if (TYPE == 81) {
+            double X2, Y2, Z2;
+            mdci05_terms(h, u, uu, v, vv, vq, rem2, h.rcut2, h.tsr_t, X2, Y2, Z2);
+            X -= X2;
+            Y -= Y2;
+            Z -= Z2;
+        }
+        rotate_acc(h, h.pref_h * X, h.pref_h * Y, h.pref_h * Z, w, acc);
+    }
+}
+
+/* ----------------------------------------------------------------- potential ---- */
+
+struct Cpx {
+    double re, im;
+};
+__device__ __forceinline__ Cpx cmul(Cpx a, Cpx b) { return {a.re * b.re - a.im * b.im, a.im * b.re + b.im * a.re}; }
+/* a/b, zero when |b| = 0 (dcpx_GPU, src/lt_math_GPU.cuh:224-243) */
+__device__ __forceinline__ Cpx cdiv(Cpx a, Cpx b)
+{
+    double n = b.re * b.re + b.im * b.im;
+    if (n == 0.) return {0., 0.};
+    double in = 1.0 / n;
+    return {(a.re * b.re + a.im * b.im) * in, (a.im * b.re - a.re * b.im) * in};
+}
+__device__ __forceinline__ Cpx clog(Cpx a) { return {0.5 * log(a.re * a.re + a.im * a.im), atan2(a.im, a.re)}; }
+
+/* cosh of (re, im) given cos(im), sin(im) (coshcpx_GPU, src/lt_math_GPU.cuh:297-307). */
+__device__ __forceinline__ Cpx ccosh_cs(double re, double c, double s)
+{
+    double ep = exp(re), em = exp(-re);
+    return {0.5 * (ep + em) * c, 0.5 * (ep - em) * s};
+}
+
+/* One pi05 term without its prefactor b0 ci / sqrt(rem2): r (Im(ckk) x - Re(ckk) y).
+ * eta, cosh(eta)^2 and sinh(2 eta) depend only on the pixel and are shared by the
+ * core and cut radii. */
+__device__ __forceinline__ double pi05_core(double u, double v, double srem, double rem2, double r, double r2,
+                                            double eta_re, double ce, double se, Cpx ch2, Cpx sh2e)
+{
+    double zr = 0.5 * log((srem + sqrt(r2 + rem2)) / r);
+    Cpx b1 = ccosh_cs(eta_re + zr, ce, se);
+    Cpx b2 = ccosh_cs(eta_re - zr, ce, se);
+    Cpx a1 = clog(cdiv(ch2, cmul(b1, b2)));
+    Cpx a2 = clog(cdiv(b1, b2));
+    double ez = exp(2. * zr), emz = exp(-2. * zr);
+    Cpx sh2z = {0.5 * (ez - emz), 0.};
+    Cpx c1 = cmul(sh2e, a1);
+    Cpx c2 = cmul(sh2z, a2);
+    double kre = c1.re + c2.re, kim = c1.im + c2.im;
+    return r * (kim * u - kre * v);
+}
+
+template <int TYPE>
+__device__ __forceinline__ void pot_pair(const lt_rec64 &h, double px, double py, double &psi)
+{
+    Frame64 f = to_frame(h, px, py);
+    double u = f.u, v = f.v;
+    double uu = u * u, vv = v * v;
+    if (TYPE == 5) {
+        psi += h.b0 * sqrt(uu * h.cx1 + vv * h.cx1inv);
+        return;
+    }
+    double rem2 = uu * h.cxro_inv + vv * h.cyro_inv;
+    double srem = sqrt(rem2);
+    double z = sqrt(uu + vv);
+    double eta_re = -.5 * asinh(h.e1 * v / z);
+    double eta_im = .5 * asin(h.e2 * u / z);
+    double se, ce;
+    sincos(eta_im, &se, &ce);
+    Cpx ch = ccosh_cs(eta_re, ce, se);
+    Cpx ch2 = {ch.re * ch.re - ch.im * ch.im, 2. * ch.re * ch.im};
+    double s2, c2;
+    sincos(2. * eta_im, &s2, &c2);
+    double e2p = exp(2. * eta_re), e2m = exp(-2. * eta_re);
+    Cpx sh2e = {0.5 * (e2p - e2m) * c2, 0.5 * (e2p + e2m) * s2};
+    double t = pi05_core(u, v, srem, rem2, h.rc, h.rc2, eta_re, ce, se, ch2, sh2e);
+    if (TYPE == 81) t -= pi05_core(u, v, srem, rem2, h.rcut, h.rcut2, eta_re, ce, se, ch2, sh2e);
+    psi += h.pref_h * t / srem;
+}
+
+} // namespace lt

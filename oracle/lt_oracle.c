@@ -1,0 +1,581 @@
+/*
+ * lt_oracle.c -- CPU restatement of Lenstool-HPC's lensing-map arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker: tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline leg may call it; the product library never links it.
+ *
+ * Every function cites the reference lines it restates (paths relative to the
+ * Lenstool-HPC source tree).  The per-pair arithmetic keeps the reference's operation
+ * order so that FP64 results agree to rounding.  Three pieces have no reference
+ * source and are restated from the mathematics (parity for them is pinned by finite
+ * differences of the reference-backed pieces, see tests/test_oracle.py):
+ *   - SIS Hessian (derivative of src/gradient.cpp:260-299),
+ *   - PIEMD Hessian (one mdci05 term, src/gradient2.cpp:54-83, without the cut),
+ *   - SIS and PIEMD potential (SIS: b0*R; PIEMD: one pi05 term).
+ *
+ * Halo catalogue: the Potential_SOA field meaning of src/structure_hpc.hpp:257-287,
+ * sorted into runs of equal type (src/module_readParameters.cpp:2289-2293).  Unlike
+ * the reference, no sentinel slot type[n] is read.
+ */
+#include <math.h>
+#include <stddef.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef struct {
+    int n;
+    const int *type;
+    const double *x, *y;     /* position_x, position_y */
+    const double *cs, *sn;   /* anglecos, anglesin */
+    const double *eps;       /* ellipticity_potential */
+    const double *rc, *rcut; /* rcore, rcut */
+    const double *b0;        /* impact parameter */
+    const double *dlsds;     /* per-halo D_LS/D_OS (Kmap weights); may be NULL */
+} lto_cat;
+
+typedef struct {
+    double xmin, ymin, dx, dy;
+    int nx, ny, istart, jstart;
+} lto_grid;
+
+enum { LTO_OK = 0, LTO_ERR_PROFILE = 2, LTO_ERR_ARG = 1 };
+
+/* ---------------------------------------------------------------------------------- */
+/* gradient                                                                           */
+/* ---------------------------------------------------------------------------------- */
+
+/* SIS deflection of halo i, src/gradient.cpp:260-299 (the _v2 variant).  The inverse
+ * radius starts from a single-precision square root followed by one Newton step
+ * (src/gradient.cpp:287-288). */
+static void sis_grad_acc(const lto_cat *c, int i, double px, double py, double *gx, double *gy)
+{
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double b0 = c->b0[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    double u = tx * cs + ty * sn;
+    double v = ty * cs - tx * sn;
+    double e = c->eps[i];
+    double q = u * u * (1. - e) + v * v * (1. + e);
+    double r = 1. / sqrtf((float)q);
+    r = r * (1.5 - 0.5 * q * r * r);
+    double fx = (1. - e) * b0 * u * r;
+    double fy = (1. + e) * b0 * v * r;
+    *gx += fx * cs - fy * sn;
+    *gy += fy * cs + fx * sn;
+}
+
+/* One complex-logarithm term of the PIEMD deflection for core radius r: the KERNEL
+ * macro of src/gradient.hpp:64-76 (also piemd_1derivatives_ci05, src/gradient.cpp:60-100). */
+static void piemd_term(double u, double v, double r, double sqe, double cx1, double rem2,
+                       double zci_im, double *re, double *im)
+{
+    double nre = cx1 * u;
+    double nim = 2. * sqe * sqrt(r * r + rem2) - v / cx1;
+    double dim = 2. * r * sqe - v;
+    double nrm = (u * u + dim * dim);
+    double zre = (nre * u + nim * dim) / nrm;
+    double zim = (nim * u - nre * dim) / nrm;
+    double m = zre;
+    double lre = log(sqrt(m * m + zim * zim));
+    double lim = atan2(zim, m);
+    *re = -zci_im * lim;
+    *im = zci_im * lre;
+}
+
+/* PIEMD deflection, src/gradient.cpp:548-607. */
+static void piemd_grad_acc(const lto_cat *c, int i, double px, double py, double *gx, double *gy)
+{
+    double b0 = c->b0[i];
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    double u = tx * cs + ty * sn;
+    double v = ty * cs - tx * sn;
+    double e = c->eps[i];
+    double rc = c->rc[i];
+    double sqe = sqrt(e);
+    double cx1 = (1. - e) / (1. + e);
+    double cxro = (1. + e) * (1. + e);
+    double cyro = (1. - e) * (1. - e);
+    double rem2 = u * u / cxro + v * v / cyro;
+    double zci_im = -0.5 * (1. - e * e) / sqe;
+    double re, im;
+    piemd_term(u, v, rc, sqe, cx1, rem2, zci_im, &re, &im);
+    *gx += b0 * (re * cs - im * sn);
+    *gy += b0 * (im * cs + re * sn);
+}
+
+/* Cut dPIE deflection, src/gradient.cpp:744-811: t05 * (K(rcore) - K(rcut)). */
+static void dpie_grad_acc(const lto_cat *c, int i, double px, double py, double *gx, double *gy)
+{
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    double u = tx * cs + ty * sn;
+    double v = ty * cs - tx * sn;
+    double e = c->eps[i];
+    double rc = c->rc[i], rcut = c->rcut[i], b0 = c->b0[i];
+    double t05 = b0 * rcut / (rcut - rc);
+    double sqe = sqrt(e);
+    double cx1 = (1. - e) / (1. + e);
+    double cxro = (1. + e) * (1. + e);
+    double cyro = (1. - e) * (1. - e);
+    double rem2 = u * u / cxro + v * v / cyro;
+    double zci_im = -0.5 * (1. - e * e) / sqe;
+    double are, aim, bre, bim;
+    piemd_term(u, v, rc, sqe, cx1, rem2, zci_im, &are, &aim);
+    piemd_term(u, v, rcut, sqe, cx1, rem2, zci_im, &bre, &bim);
+    double zre = t05 * (are - bre);
+    double zim = t05 * (aim - bim);
+    *gx += (zre * cs - zim * sn);
+    *gy += (zim * cs + zre * sn);
+}
+
+/* Sum over halos at one point, dispatched over runs of equal type:
+ * module_potentialDerivatives_totalGradient_SOA, src/gradient.cpp:899-929.  Each run is
+ * summed on its own and then added to the total, as the reference does. */
+static int grad_point(const lto_cat *c, double px, double py, double *ax, double *ay)
+{
+    double tx = 0., ty = 0.;
+    int s = 0;
+    while (s < c->n) {
+        int t = c->type[s];
+        int e = s + 1;
+        while (e < c->n && c->type[e] == t) e++;
+        double rx = 0., ry = 0.;
+        switch (t) {
+        case 5:  for (int i = s; i < e; i++) sis_grad_acc(c, i, px, py, &rx, &ry); break;
+        case 8:  for (int i = s; i < e; i++) piemd_grad_acc(c, i, px, py, &rx, &ry); break;
+        case 81: for (int i = s; i < e; i++) dpie_grad_acc(c, i, px, py, &rx, &ry); break;
+        default: return LTO_ERR_PROFILE;
+        }
+        tx += rx;
+        ty += ry;
+        s = e;
+    }
+    *ax = tx;
+    *ay = ty;
+    return LTO_OK;
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* Hessian                                                                            */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct { double a, b, c, d; } lto_mat;
+
+/* Second derivatives of one PIEMD term I0.5 (Kassiola & Kovner 1993):
+ * mdci05_hpc, src/gradient2.cpp:54-83. */
+static lto_mat mdci05(double x, double y, double eps, double rc, double b0)
+{
+    double sqe = sqrt(eps);
+    double cx1 = (1. - eps) / (1. + eps);
+    double cx1inv = 1. / cx1;
+    double cxro = (1. + eps) * (1. + eps);
+    double cyro = (1. - eps) * (1. - eps);
+    double ci = 0.5 * (1. - eps * eps) / sqe;
+    double wrem = sqrt(rc * rc + x * x / cxro + y * y / cyro);
+    double den1 = 2. * sqe * wrem - y * cx1inv;
+    den1 = cx1 * cx1 * x * x + den1 * den1;
+    double num2 = 2. * rc * sqe - y;
+    double den2 = x * x + num2 * num2;
+    double didxre = ci * (cx1 * (2. * sqe * x * x / cxro / wrem - 2. * sqe * wrem + y * cx1inv) / den1 + num2 / den2);
+    double didyre = ci * ((2. * sqe * x * y * cx1 / cyro / wrem - x) / den1 + x / den2);
+    double didyim = ci * ((2. * sqe * wrem * cx1inv - y * cx1inv * cx1inv - 4. * eps * y / cyro +
+                           2. * sqe * y * y / cyro / wrem * cx1inv) / den1 - num2 / den2);
+    lto_mat r;
+    r.a = b0 * didxre;
+    r.b = r.d = b0 * didyre;
+    r.c = b0 * didyim;
+    return r;
+}
+
+/* Rotate a Hessian from the halo frame back to the sky frame, H = R^T H' R, with the
+ * two-step order of src/gradient2.cpp:146-156. */
+static void rotate_back_acc(lto_mat h, double cs, double sn, lto_mat *acc)
+{
+    lto_mat m;
+    m.a = h.a * cs + h.b * -sn;
+    m.b = h.a * sn + h.b * cs;
+    m.c = h.d * sn + h.c * cs;
+    m.d = h.d * cs + h.c * -sn;
+    acc->a += cs * m.a - sn * m.d;
+    acc->b += cs * m.b - sn * m.c;
+    acc->c += sn * m.b + cs * m.c;
+    acc->d += sn * m.a + cs * m.d;
+}
+
+/* dPIE Hessian, src/gradient2.cpp:92-205 (elliptical branch, taken for every halo). */
+static void dpie_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat *acc)
+{
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    double u = tx * cs + ty * sn;
+    double v = ty * cs - tx * sn;
+    double t05 = c->rcut[i] / (c->rcut[i] - c->rc[i]);
+    lto_mat core = mdci05(u, v, c->eps[i], c->rc[i], c->b0[i]);
+    lto_mat cut = mdci05(u, v, c->eps[i], c->rcut[i], c->b0[i]);
+    core.a = t05 * (core.a - cut.a);
+    core.b = t05 * (core.b - cut.b);
+    core.c = t05 * (core.c - cut.c);
+    core.d = t05 * (core.d - cut.d);
+    rotate_back_acc(core, cs, sn, acc);
+}
+
+/* PIEMD Hessian (restated; the reference has no type-8 Hessian): one mdci05 term with
+ * impact parameter b0, the dPIE structure of src/gradient2.cpp:92-156 without the cut. */
+static void piemd_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat *acc)
+{
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    double u = tx * cs + ty * sn;
+    double v = ty * cs - tx * sn;
+    lto_mat h = mdci05(u, v, c->eps[i], c->rc[i], c->b0[i]);
+    rotate_back_acc(h, cs, sn, acc);
+}
+
+/* SIS Hessian (restated): derivative of the deflection of src/gradient.cpp:260-299.
+ * With R^2 = (1-e)u^2 + (1+e)v^2 in the halo frame:
+ *   psi_uu = b0 (1-e)(1+e) v^2 / R^3,  psi_vv = b0 (1-e)(1+e) u^2 / R^3,
+ *   psi_uv = -b0 (1-e)(1+e) u v / R^3. */
+static void sis_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat *acc)
+{
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    double u = tx * cs + ty * sn;
+    double v = ty * cs - tx * sn;
+    double e = c->eps[i];
+    double q = u * u * (1. - e) + v * v * (1. + e);
+    double r = sqrt(q);
+    double k = c->b0[i] * (1. - e) * (1. + e) / (q * r);
+    lto_mat h;
+    h.a = k * v * v;
+    h.c = k * u * u;
+    h.b = h.d = -k * u * v;
+    rotate_back_acc(h, cs, sn, acc);
+}
+
+/* Hessian at one point, run-dispatched as module_potentialDerivatives_totalGradient2_SOA
+ * (src/gradient2.cpp:226-254).  With kmap != 0 the runs also break where dlsds changes
+ * and each run is weighted by its dlsds: module_potentialDerivatives_Kmap_SOA_GPU,
+ * src/gradient2_GPU.cu:455-522. */
+static int hess_point(const lto_cat *c, double px, double py, int kmap, lto_mat *out)
+{
+    lto_mat tot = {0., 0., 0., 0.};
+    int s = 0;
+    while (s < c->n) {
+        int t = c->type[s];
+        double w = kmap ? c->dlsds[s] : 1.;
+        int e = s + 1;
+        while (e < c->n && c->type[e] == t && (!kmap || c->dlsds[e] == w)) e++;
+        lto_mat r = {0., 0., 0., 0.};
+        switch (t) {
+        case 5:  for (int i = s; i < e; i++) sis_hess_acc(c, i, px, py, &r); break;
+        case 8:  for (int i = s; i < e; i++) piemd_hess_acc(c, i, px, py, &r); break;
+        case 81: for (int i = s; i < e; i++) dpie_hess_acc(c, i, px, py, &r); break;
+        default: return LTO_ERR_PROFILE;
+        }
+        if (kmap) {
+            tot.a += r.a * w; tot.b += r.b * w; tot.c += r.c * w; tot.d += r.d * w;
+        } else {
+            tot.a += r.a; tot.b += r.b; tot.c += r.c; tot.d += r.d;
+        }
+        s = e;
+    }
+    *out = tot;
+    return LTO_OK;
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* potential                                                                          */
+/* ---------------------------------------------------------------------------------- */
+
+typedef struct { double re, im; } lto_cpx;
+
+static lto_cpx cx_add(lto_cpx a, lto_cpx b) { lto_cpx r = {a.re + b.re, a.im + b.im}; return r; }
+static lto_cpx cx_sub(lto_cpx a, lto_cpx b) { lto_cpx r = {a.re - b.re, a.im - b.im}; return r; }
+static lto_cpx cx_mul(lto_cpx a, lto_cpx b)
+{
+    lto_cpx r = {a.re * b.re - a.im * b.im, a.im * b.re + b.im * a.re};
+    return r;
+}
+static lto_cpx cx_scale(lto_cpx a, double f) { lto_cpx r = {a.re * f, a.im * f}; return r; }
+static lto_cpx cx_sq(lto_cpx a) { lto_cpx r = {a.re * a.re - a.im * a.im, 2. * a.re * a.im}; return r; }
+/* a/b, zero when |b| = 0 (dcpx_GPU, src/lt_math_GPU.cuh:224-243). */
+static lto_cpx cx_div(lto_cpx a, lto_cpx b)
+{
+    double n = b.re * b.re + b.im * b.im;
+    lto_cpx r = {0., 0.};
+    if (n != 0.) {
+        r.re = (a.re * b.re + a.im * b.im) / n;
+        r.im = (a.im * b.re - a.re * b.im) / n;
+    }
+    return r;
+}
+static lto_cpx cx_cosh(lto_cpx a)
+{
+    double ep = exp(a.re), em = exp(-a.re);
+    lto_cpx r = {0.5 * (ep + em) * cos(a.im), 0.5 * (ep - em) * sin(a.im)};
+    return r;
+}
+static lto_cpx cx_sinh(lto_cpx a)
+{
+    double ep = exp(a.re), em = exp(-a.re);
+    lto_cpx r = {0.5 * (ep - em) * cos(a.im), 0.5 * (ep + em) * sin(a.im)};
+    return r;
+}
+static lto_cpx cx_log(lto_cpx a)
+{
+    lto_cpx r = {log(sqrt(a.re * a.re + a.im * a.im)), atan2(a.im, a.re)};
+    return r;
+}
+
+/* Potential of one PIEMD term I0.5 at (x, y) in the halo frame: pi05_gpu,
+ * src/potential_GPU.cu:47-72, with the complex helpers of src/lt_math_GPU.cuh. */
+static double pi05(double x, double y, double eps, double rc, double b0)
+{
+    double sqe = sqrt(eps);
+    double ci = .5 * (1. - eps * eps) / sqe;
+    double cxro = (1. + eps) * (1. + eps);
+    double cyro = (1. - eps) * (1. - eps);
+    double rem2 = x * x / cxro + y * y / cyro;
+    double e1 = 2. * sqe / (1 - eps);
+    double e2 = 2. * sqe / (1 + eps);
+    double z = sqrt(x * x + y * y);
+    lto_cpx eta = {-.5 * asinh(e1 * y / z), .5 * asin(e2 * x / z)};
+    lto_cpx zeta = {0.5 * log((sqrt(rem2) + sqrt(rc * rc + rem2)) / rc), 0.};
+    lto_cpx b1 = cx_cosh(cx_add(eta, zeta));
+    lto_cpx b2 = cx_cosh(cx_sub(eta, zeta));
+    lto_cpx a1 = cx_log(cx_div(cx_sq(cx_cosh(eta)), cx_mul(b1, b2)));
+    lto_cpx a2 = cx_log(cx_div(b1, b2));
+    lto_cpx c1 = cx_mul(cx_sinh(cx_scale(eta, 2.)), a1);
+    lto_cpx c2 = cx_mul(cx_sinh(cx_scale(zeta, 2.)), a2);
+    lto_cpx ckk = cx_add(c1, c2);
+    return b0 * ci * rc / sqrt(rem2) * (ckk.im * x - ckk.re * y);
+}
+
+static void halo_frame(const lto_cat *c, int i, double px, double py, double *u, double *v)
+{
+    double tx = px - c->x[i], ty = py - c->y[i];
+    double cs = c->cs[i], sn = c->sn[i];
+    *u = tx * cs + ty * sn;
+    *v = ty * cs - tx * sn;
+}
+
+/* Potential at one point: module_potential_totalPotential_SOA_GPU and
+ * module_potential_81_SOA_GPU, src/potential_GPU.cu:75-187 (dPIE); SIS (b0 R) and
+ * PIEMD (one pi05 term) are restated. */
+static int pot_point(const lto_cat *c, double px, double py, double *out)
+{
+    double tot = 0.;
+    int s = 0;
+    while (s < c->n) {
+        int t = c->type[s];
+        int e = s + 1;
+        while (e < c->n && c->type[e] == t) e++;
+        double r = 0.;
+        for (int i = s; i < e; i++) {
+            double u, v;
+            halo_frame(c, i, px, py, &u, &v);
+            if (t == 81) {
+                double t05 = c->rcut[i] / (c->rcut[i] - c->rc[i]);
+                double pa = pi05(u, v, c->eps[i], c->rc[i], c->b0[i]);
+                double ps = pi05(u, v, c->eps[i], c->rcut[i], c->b0[i]);
+                r += t05 * (pa - ps);
+            } else if (t == 8) {
+                r += pi05(u, v, c->eps[i], c->rc[i], c->b0[i]);
+            } else if (t == 5) {
+                double e_ = c->eps[i];
+                r += c->b0[i] * sqrt(u * u * (1. - e_) + v * v * (1. + e_));
+            } else {
+                return LTO_ERR_PROFILE;
+            }
+        }
+        tot += r;
+        s = e;
+    }
+    *out = tot;
+    return LTO_OK;
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* grids and point lists                                                              */
+/* ---------------------------------------------------------------------------------- */
+
+/* Pixel (ii, jj) sits at xmin + (ii + istart) dx, ymin + (jj + jstart) dy and is stored
+ * at jj*nx + ii: gradient_grid_general_CPU, src/grid_gradient_CPU.cpp:67-100. */
+static void pixel_xy(const lto_grid *g, long p, double *px, double *py)
+{
+    int ii = (int)(p % g->nx), jj = (int)(p / g->nx);
+    *px = g->xmin + (ii + g->istart) * g->dx;
+    *py = g->ymin + (jj + g->jstart) * g->dy;
+}
+
+static void set_threads(int nthreads)
+{
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+}
+
+int lto_grad_grid(const lto_cat *c, const lto_grid *g, double *ax, double *ay, int nthreads)
+{
+    long np = (long)g->nx * g->ny;
+    int bad = 0;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+    for (long p = 0; p < np; p++) {
+        double px, py;
+        pixel_xy(g, p, &px, &py);
+        bad |= grad_point(c, px, py, &ax[p], &ay[p]);
+    }
+    return bad;
+}
+
+int lto_hess_grid(const lto_cat *c, const lto_grid *g, int kmap, double *a, double *b,
+                  double *cc, double *d, int nthreads)
+{
+    long np = (long)g->nx * g->ny;
+    int bad = 0;
+    if (kmap && !c->dlsds) return LTO_ERR_ARG;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+    for (long p = 0; p < np; p++) {
+        double px, py;
+        lto_mat m;
+        pixel_xy(g, p, &px, &py);
+        bad |= hess_point(c, px, py, kmap, &m);
+        a[p] = m.a; b[p] = m.b; cc[p] = m.c; d[p] = m.d;
+    }
+    return bad;
+}
+
+int lto_pot_grid(const lto_cat *c, const lto_grid *g, double *psi, int nthreads)
+{
+    long np = (long)g->nx * g->ny;
+    int bad = 0;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+    for (long p = 0; p < np; p++) {
+        double px, py;
+        pixel_xy(g, p, &px, &py);
+        bad |= pot_point(c, px, py, &psi[p]);
+    }
+    return bad;
+}
+
+/* Point-list forms: the same sums at arbitrary (px[k], py[k]). */
+int lto_grad_points(const lto_cat *c, long np, const double *px, const double *py,
+                    double *ax, double *ay, int nthreads)
+{
+    int bad = 0;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+    for (long k = 0; k < np; k++) bad |= grad_point(c, px[k], py[k], &ax[k], &ay[k]);
+    return bad;
+}
+
+int lto_hess_points(const lto_cat *c, long np, const double *px, const double *py, int kmap,
+                    double *a, double *b, double *cc, double *d, int nthreads)
+{
+    int bad = 0;
+    if (kmap && !c->dlsds) return LTO_ERR_ARG;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+    for (long k = 0; k < np; k++) {
+        lto_mat m;
+        bad |= hess_point(c, px[k], py[k], kmap, &m);
+        a[k] = m.a; b[k] = m.b; cc[k] = m.c; d[k] = m.d;
+    }
+    return bad;
+}
+
+int lto_pot_points(const lto_cat *c, long np, const double *px, const double *py, double *psi,
+                   int nthreads)
+{
+    int bad = 0;
+    set_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
+    for (long k = 0; k < np; k++) bad |= pot_point(c, px[k], py[k], &psi[k]);
+    return bad;
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* map epilogues                                                                      */
+/* ---------------------------------------------------------------------------------- */
+
+/* Eigenvalues of the symmetric 2x2 matrix [[a, b], [b, c]]: formeli_ampli,
+ * src/grid_map_ampli_GPU.cu:549-572 (the orientation is not used by any map). */
+static void eigen2(double a, double b, double c, double *lam, double *mu)
+{
+    double delta = (a - c) * (a - c) + 4 * b * b;
+    double e = sqrt(delta);
+    *lam = .5 * (a + c + e);
+    *mu = .5 * (a + c - e);
+}
+
+/* Map kinds (one plane each). */
+enum {
+    LTO_MAP_AMPLI1 = 1, LTO_MAP_AMPLI2, LTO_MAP_AMPLI3, LTO_MAP_AMPLI4, LTO_MAP_AMPLI5, LTO_MAP_AMPLI6,
+    LTO_MAP_SHEAR1 = 11, LTO_MAP_SHEAR2, LTO_MAP_SHEAR3, LTO_MAP_SHEAR4,
+    LTO_MAP_KAPPA = 21, LTO_MAP_GAMMA1, LTO_MAP_GAMMA2, LTO_MAP_MU, LTO_MAP_SCALE
+};
+
+/* One derived map from the Hessian planes, D = dls/ds.
+ *  ampli 1-6: src/grid_map_ampli_GPU.cu:329-547;  shear 1-4: src/grid_map_shear_GPU.cu:208-369;
+ *  kappa/gamma1/gamma2/mu: the D-scaled convergence, shear components and
+ *  magnification 1/((1-k)^2 - g1^2 - g2^2);
+ *  LTO_MAP_SCALE: (a + c)/2 * scale (mass maps, src/grid_map_mass_GPU.cu:307-322). */
+int lto_map(int kind, long np, const double *a, const double *b, const double *c, double D,
+            double scale, double *out)
+{
+    for (long p = 0; p < np; p++) {
+        double A = 1. - a[p] * D, B = -b[p] * D, C = 1. - c[p] * D;
+        double lam, mu, r;
+        switch (kind) {
+        case LTO_MAP_AMPLI1: eigen2(A, B, C, &lam, &mu); r = 1. / (lam * mu); break;
+        case LTO_MAP_AMPLI2: eigen2(A, B, C, &lam, &mu); r = 1. / fabs(lam * mu); break;
+        case LTO_MAP_AMPLI3: eigen2(A, B, C, &lam, &mu); r = -2.5 * log10(fabs(lam * mu)); break;
+        case LTO_MAP_AMPLI4: {
+            double k = (a[p] + c[p]) * D / 2.;
+            double g1 = (a[p] - c[p]) * D / 2.;
+            double g2 = b[p] * D;
+            double g = sqrt(g1 * g1 + g2 * g2);
+            double gp = g / (1 - k);
+            r = (1 - k) * (1 + gp * gp) / (1 - gp * gp);
+            break;
+        }
+        case LTO_MAP_AMPLI5: r = (a[p] + c[p]) / 2.; break;
+        case LTO_MAP_AMPLI6: {
+            double g1 = (a[p] - c[p]) / 2.;
+            double g2 = b[p];
+            r = sqrt(g1 * g1 + g2 * g2);
+            break;
+        }
+        case LTO_MAP_SHEAR1: eigen2(A, B, C, &lam, &mu); r = (lam - mu) / 2.; break;
+        case LTO_MAP_SHEAR2: {
+            eigen2(A, B, C, &lam, &mu);
+            double q = lam / mu;
+            r = fabs((q * q - 1.) / (q * q + 1.));
+            break;
+        }
+        case LTO_MAP_SHEAR3: r = (a[p] - c[p]) * D / 2.; break;
+        case LTO_MAP_SHEAR4: r = b[p] * D; break;
+        case LTO_MAP_KAPPA: r = (a[p] + c[p]) * D / 2.; break;
+        case LTO_MAP_GAMMA1: r = (a[p] - c[p]) * D / 2.; break;
+        case LTO_MAP_GAMMA2: r = b[p] * D; break;
+        case LTO_MAP_MU: {
+            double k = (a[p] + c[p]) * D / 2.;
+            double g1 = (a[p] - c[p]) * D / 2.;
+            double g2 = b[p] * D;
+            r = 1. / ((1. - k) * (1. - k) - g1 * g1 - g2 * g2);
+            break;
+        }
+        case LTO_MAP_SCALE: r = (a[p] + c[p]) * 0.5 * scale; break;
+        default: return LTO_ERR_ARG;
+        }
+        out[p] = r;
+    }
+    return LTO_OK;
+}

@@ -1,0 +1,221 @@
+"""ctypes bindings of the checker libraries (TEST INFRASTRUCTURE ONLY).
+
+``Oracle``  -> liblt_oracle.so, the C restatement in lt_oracle.c.
+``RefLib``  -> _ref/libltref.so, the reference's own code (built here from the reference
+               sources by oracle/Makefile; the built .so travels with the repository).
+
+A catalogue is any object with the Potential_SOA arrays as attributes: ``type`` (int32)
+and position_x, position_y, anglecos, anglesin, ellipticity_potential, rcore, rcut, b0,
+dlsds (float64), sorted into runs of equal type.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+import subprocess
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ORACLE_SO = HERE / "liblt_oracle.so"
+REF_SO = HERE / "_ref" / "libltref.so"
+REFERENCE_TREE = pathlib.Path("/root/reference")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def build(with_reference: bool | None = None) -> None:
+    """Compile the oracle, and the reference library when the reference tree exists."""
+    subprocess.run(["make", "-s", "oracle"], cwd=HERE, check=True)
+    if with_reference is None:
+        with_reference = (REFERENCE_TREE / "src" / "gradient.cpp").exists()
+    if with_reference:
+        subprocess.run(["make", "-s", "ref", f"REF={REFERENCE_TREE}"], cwd=HERE, check=True)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+class _Cat(C.Structure):
+    _fields_ = [("n", C.c_int), ("type", _ip)] + [(f, _dp) for f in
+                                                ("x", "y", "cs", "sn", "eps", "rc", "rcut", "b0", "dlsds")]
+
+
+class _Grid(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("ymin", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+                ("nx", C.c_int), ("ny", C.c_int), ("istart", C.c_int), ("jstart", C.c_int)]
+
+
+def _arrays(cat):
+    t = np.ascontiguousarray(cat.type, dtype=np.int32)
+    fl = [np.ascontiguousarray(getattr(cat, f), dtype=np.float64) for f in
+          ("position_x", "position_y", "anglecos", "anglesin", "ellipticity_potential", "rcore", "rcut", "b0",
+           "dlsds")]
+    return t, fl
+
+
+# map kinds of lto_map()
+MAP_KINDS = {"ampli1": 1, "ampli2": 2, "ampli3": 3, "ampli4": 4, "ampli5": 5, "ampli6": 6,
+             "shear1": 11, "shear2": 12, "shear3": 13, "shear4": 14,
+             "kappa": 21, "gamma1": 22, "gamma2": 23, "mu": 24, "scale": 25}
+
+
+class Oracle:
+    """The C restatement.  All results are float64 numpy arrays."""
+
+    def __init__(self, path=ORACLE_SO, threads: int = 0):
+        if not pathlib.Path(path).exists():
+            build(with_reference=False)
+        self.lib = C.CDLL(str(path))
+        self.threads = threads or os.cpu_count()
+        L = self.lib
+        L.lto_grad_grid.argtypes = [C.POINTER(_Cat), C.POINTER(_Grid), _dp, _dp, C.c_int]
+        L.lto_hess_grid.argtypes = [C.POINTER(_Cat), C.POINTER(_Grid), C.c_int, _dp, _dp, _dp, _dp, C.c_int]
+        L.lto_pot_grid.argtypes = [C.POINTER(_Cat), C.POINTER(_Grid), _dp, C.c_int]
+        L.lto_grad_points.argtypes = [C.POINTER(_Cat), C.c_long, _dp, _dp, _dp, _dp, C.c_int]
+        L.lto_hess_points.argtypes = [C.POINTER(_Cat), C.c_long, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp, C.c_int]
+        L.lto_pot_points.argtypes = [C.POINTER(_Cat), C.c_long, _dp, _dp, _dp, C.c_int]
+        L.lto_map.argtypes = [C.c_int, C.c_long, _dp, _dp, _dp, C.c_double, C.c_double, _dp]
+
+    def _cat(self, cat):
+        t, fl = _arrays(cat)
+        s = _Cat(int(t.shape[0]), t.ctypes.data_as(_ip), *[_d(a) for a in fl])
+        return s, (t, fl)
+
+    @staticmethod
+    def _grid(g):
+        return _Grid(g.xmin, g.ymin, g.dx, g.dy, g.nx, g.ny, g.istart, g.jstart)
+
+    @staticmethod
+    def _check(rc):
+        if rc != 0:
+            raise ValueError(f"oracle error {rc} (unknown profile type or bad argument)")
+
+    def grad_grid(self, cat, g):
+        s, keep = self._cat(cat)
+        ax = np.empty(g.nx * g.ny); ay = np.empty(g.nx * g.ny)
+        self._check(self.lib.lto_grad_grid(C.byref(s), C.byref(self._grid(g)), _d(ax), _d(ay), self.threads))
+        return ax.reshape(g.ny, g.nx), ay.reshape(g.ny, g.nx)
+
+    def hess_grid(self, cat, g, kmap=False):
+        s, keep = self._cat(cat)
+        out = [np.empty(g.nx * g.ny) for _ in range(4)]
+        self._check(self.lib.lto_hess_grid(C.byref(s), C.byref(self._grid(g)), int(kmap), *[_d(o) for o in out],
+                                           self.threads))
+        return tuple(o.reshape(g.ny, g.nx) for o in out)
+
+    def pot_grid(self, cat, g):
+        s, keep = self._cat(cat)
+        psi = np.empty(g.nx * g.ny)
+        self._check(self.lib.lto_pot_grid(C.byref(s), C.byref(self._grid(g)), _d(psi), self.threads))
+        return psi.reshape(g.ny, g.nx)
+
+    def grad_points(self, cat, px, py):
+        s, keep = self._cat(cat)
+        px = np.ascontiguousarray(px, np.float64); py = np.ascontiguousarray(py, np.float64)
+        ax = np.empty_like(px); ay = np.empty_like(px)
+        self._check(self.lib.lto_grad_points(C.byref(s), px.size, _d(px), _d(py), _d(ax), _d(ay), self.threads))
+        return ax, ay
+
+    def hess_points(self, cat, px, py, kmap=False):
+        s, keep = self._cat(cat)
+        px = np.ascontiguousarray(px, np.float64); py = np.ascontiguousarray(py, np.float64)
+        out = [np.empty_like(px) for _ in range(4)]
+        self._check(self.lib.lto_hess_points(C.byref(s), px.size, _d(px), _d(py), int(kmap), *[_d(o) for o in out],
+                                             self.threads))
+        return tuple(out)
+
+    def pot_points(self, cat, px, py):
+        s, keep = self._cat(cat)
+        px = np.ascontiguousarray(px, np.float64); py = np.ascontiguousarray(py, np.float64)
+        psi = np.empty_like(px)
+        self._check(self.lib.lto_pot_points(C.byref(s), px.size, _d(px), _d(py), _d(psi), self.threads))
+        return psi
+
+    def map(self, kind, a, b, c, D=1., scale=1.):
+        a = np.ascontiguousarray(a, np.float64).ravel()
+        b = np.ascontiguousarray(b, np.float64).ravel()
+        c = np.ascontiguousarray(c, np.float64).ravel()
+        out = np.empty_like(a)
+        self._check(self.lib.lto_map(MAP_KINDS[kind], a.size, _d(a), _d(b), _d(c), D, scale, _d(out)))
+        return out
+
+
+class RefLib:
+    """The reference's own CPU code (and GPU kernels compiled for the host)."""
+
+    def __init__(self, path=REF_SO):
+        if not pathlib.Path(path).exists():
+            raise FileNotFoundError(f"{path} not built (oracle/Makefile target 'ref')")
+        self.lib = C.CDLL(str(path))
+        soa = [C.c_int, _ip] + [_dp] * 9
+        L = self.lib
+        L.ltref_grad_grid.argtypes = soa + [C.c_double] * 4 + [C.c_int] * 4 + [_dp, _dp]
+        L.ltref_hess_grid.argtypes = soa + [C.c_double] * 4 + [C.c_int] * 4 + [_dp] * 4
+        L.ltref_amplif5_grid.argtypes = soa + [C.c_double] * 4 + [C.c_int, _dp]
+        L.ltref_grad_points.argtypes = soa + [C.c_long, _dp, _dp, _dp, _dp]
+        L.ltref_hess_points.argtypes = soa + [C.c_long, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ltref_pot81_points.argtypes = soa + [C.c_long, _dp, _dp, _dp]
+        L.ltref_gpu_kernel_grid.argtypes = [C.c_int] + soa + [C.c_double] * 4 + [C.c_int] * 4 + [_dp] * 4
+
+    @staticmethod
+    def _soa(cat):
+        t, fl = _arrays(cat)
+        # argument order of ref_wrap.cpp: x, y, cs, sn, eps, rc, rcut, b0, dlsds
+        return [int(t.shape[0]), t.ctypes.data_as(_ip)] + [_d(a) for a in fl], (t, fl)
+
+    def grad_grid(self, cat, g):
+        s, keep = self._soa(cat)
+        ax = np.empty(g.nx * g.ny); ay = np.empty(g.nx * g.ny)
+        self.lib.ltref_grad_grid(*s, g.xmin, g.ymin, g.dx, g.dy, g.nx, g.ny, g.istart, g.jstart, _d(ax), _d(ay))
+        return ax.reshape(g.ny, g.nx), ay.reshape(g.ny, g.nx)
+
+    def hess_grid(self, cat, g):
+        s, keep = self._soa(cat)
+        out = [np.empty(g.nx * g.ny) for _ in range(4)]
+        self.lib.ltref_hess_grid(*s, g.xmin, g.ymin, g.dx, g.dy, g.nx, g.ny, g.istart, g.jstart,
+                                 *[_d(o) for o in out])
+        return tuple(o.reshape(g.ny, g.nx) for o in out)
+
+    def amplif5_grid(self, cat, g):
+        s, keep = self._soa(cat)
+        out = np.empty(g.nx * g.nx)
+        self.lib.ltref_amplif5_grid(*s, g.xmin, g.xmax, g.ymin, g.ymax, g.nx, _d(out))
+        return out.reshape(g.nx, g.nx)
+
+    def grad_points(self, cat, px, py):
+        s, keep = self._soa(cat)
+        px = np.ascontiguousarray(px, np.float64); py = np.ascontiguousarray(py, np.float64)
+        ax = np.empty_like(px); ay = np.empty_like(px)
+        self.lib.ltref_grad_points(*s, px.size, _d(px), _d(py), _d(ax), _d(ay))
+        return ax, ay
+
+    def hess_points(self, cat, px, py):
+        s, keep = self._soa(cat)
+        px = np.ascontiguousarray(px, np.float64); py = np.ascontiguousarray(py, np.float64)
+        out = [np.empty_like(px) for _ in range(4)]
+        self.lib.ltref_hess_points(*s, px.size, _d(px), _d(py), *[_d(o) for o in out])
+        return tuple(out)
+
+    def pot81_points(self, cat, px, py):
+        s, keep = self._soa(cat)
+        px = np.ascontiguousarray(px, np.float64); py = np.ascontiguousarray(py, np.float64)
+        psi = np.empty_like(px)
+        rc = self.lib.ltref_pot81_points(*s, px.size, _d(px), _d(py), _d(psi))
+        if rc:
+            raise ValueError("the reference potential exists for type 81 only")
+        return psi
+
+    def gpu_kernel_grid(self, which, cat, g):
+        """Run a reference GPU grid kernel on the host: which = 'pot', 'hess' or 'kmap'."""
+        s, keep = self._soa(cat)
+        out = [np.zeros(g.nx * g.ny) for _ in range(4)]
+        code = {"pot": 0, "hess": 1, "kmap": 2}[which]
+        self.lib.ltref_gpu_kernel_grid(code, *s, g.xmin, g.ymin, g.dx, g.dy, g.nx, g.ny, g.istart, g.jstart,
+                                       *[_d(o) for o in out])
+        if which == "pot":
+            return out[0].reshape(g.ny, g.nx)
+        return tuple(o.reshape(g.ny, g.nx) for o in out)

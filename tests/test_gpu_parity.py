@@ -1,0 +1,208 @@
+"""FP64 parity of the CUDA path (through the C ABI) with the reference's golden vectors
+and the oracle.  Tolerance: |gpu - ref| <= 1e-12 * max(|ref|, RMS(map)) per pixel."""
+import numpy as np
+import pytest
+
+from conftest import catalog_from_npz, golden, grid_from_npz, max_rel_err
+
+import lenstool_hpc_b200 as lt
+from lenstool_hpc_b200 import catalog
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lenstool_hpc_b200 import build
+    build.build()
+    c = lt.Context(0)
+    yield c
+    c.close()
+
+
+def test_kat_dpie95(ctx):
+    z = golden("kat_dpie95.npz")
+    cat = catalog_from_npz(z)
+    px, py = float(z["px"]), float(z["py"])
+    g = catalog.Grid(px, px + 1., py, py + 1., 1, 1, dx=1., dy=1.)
+    ax, ay = ctx.gradient_grid(cat, g)
+    want = z["lenstool_grad"]
+    assert abs(ax[0, 0] - want[0]) <= 1e-12 * abs(want[0])
+    assert abs(ay[0, 0] - want[1]) <= 1e-12 * abs(want[1])
+
+
+@pytest.mark.parametrize("name", ["90Pot81", "90Pot", "90PotSIS", "MarkusBenchmark"])
+def test_par_gradient(ctx, name):
+    z = golden(f"par_{name}.npz")
+    cat, g = catalog_from_npz(z), grid_from_npz(z)
+    ax, ay = ctx.gradient_grid(cat, g)
+    assert max_rel_err(ax, z["grad"][0]) <= TOL
+    assert max_rel_err(ay, z["grad"][1]) <= TOL
+
+
+def test_par_dpie_hessian_potential_kmap(ctx):
+    z = golden("par_90Pot81.npz")
+    cat, g = catalog_from_npz(z), grid_from_npz(z)
+    m = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "hess_d", "ampli5"])
+    for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
+        assert max_rel_err(m[name], z["hess"][k]) <= TOL
+    assert max_rel_err(m["ampli5"], z["amplif5"]) <= TOL
+    psi = ctx.potential_grid(cat, g)
+    assert max_rel_err(psi, z["pot"]) <= TOL
+    kcat = catalog_from_npz(z)
+    kcat.dlsds = np.array(z["kmap_dlsds"])
+    mk = ctx.hessian_maps(kcat, g, ["hess_a", "hess_b", "hess_c", "hess_d"], kmap=True)
+    for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
+        assert max_rel_err(mk[name], z["kmap"][k]) <= TOL
+
+
+def _cat(cluster_type=81, n_gal=198, seed=20261203):
+    return catalog.cluster_galaxy_catalog(2, n_gal, seed, cluster_type=cluster_type)
+
+
+@pytest.mark.parametrize("cluster_type", [81, 8, 5])
+@pytest.mark.parametrize("shape", [(128, 96, 0, 0), (77, 51, 3, 5), (1, 1, 0, 0), (130, 9, 0, 2)])
+def test_grid_vs_oracle(ctx, oracle_lib, cluster_type, shape):
+    nx, ny, i0, j0 = shape
+    cat = _cat(cluster_type, n_gal=60)
+    g = catalog.Grid(-100., 100., -90., 80., nx, ny, i0, j0, dx=200. / 127, dy=170. / 95)
+    ax, ay = ctx.gradient_grid(cat, g)
+    ox, oy = oracle_lib.grad_grid(cat, g)
+    assert max_rel_err(ax, ox) <= TOL and max_rel_err(ay, oy) <= TOL
+    h = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "hess_d"])
+    oh = oracle_lib.hess_grid(cat, g)
+    for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
+        assert max_rel_err(h[name], oh[k]) <= TOL, name
+    psi = ctx.potential_grid(cat, g)
+    assert max_rel_err(psi, oracle_lib.pot_grid(cat, g)) <= TOL
+
+
+def test_every_map_kind_vs_oracle(ctx, oracle_lib):
+    cat = _cat(81, n_gal=80)
+    g = catalog.Grid.square(60., 64)
+    D = 0.62
+    a, b, c, d = oracle_lib.hess_grid(cat, g)
+    kinds = ["ampli1", "ampli2", "ampli3", "ampli4", "ampli5", "ampli6", "shear1", "shear2"]
+    m = ctx.hessian_maps(cat, g, kinds, dlsds=D)
+    for k in kinds:
+        assert max_rel_err(m[k], oracle_lib.map(k, a, b, c, D).reshape(g.ny, g.nx)) <= 1e-10, k
+    kinds = ["shear3", "shear4", "kappa", "gamma1", "gamma2", "mu", "mass"]
+    m = ctx.hessian_maps(cat, g, kinds, dlsds=D, mult=3.5)
+    for k in kinds:
+        ref = oracle_lib.map("scale" if k == "mass" else k, a, b, c, D, 3.5).reshape(g.ny, g.nx)
+        assert max_rel_err(m[k], ref) <= 1e-10, k
+
+
+def test_lens_maps_fused_equals_separate(ctx, oracle_lib):
+    cat = _cat(81, n_gal=100)
+    g = catalog.Grid.square(150., 96)
+    D = 0.7
+    out = ctx.lens_maps(cat, g, dlsds=D)
+    a, b, c, d = oracle_lib.hess_grid(cat, g)
+    for k in ("kappa", "gamma1", "gamma2", "mu"):
+        assert max_rel_err(out[k], oracle_lib.map(k, a, b, c, D).reshape(g.ny, g.nx)) <= 1e-10, k
+    assert max_rel_err(out["psi"], D * oracle_lib.pot_grid(cat, g)) <= TOL
+
+
+def test_device_outputs_and_stream(ctx, oracle_lib):
+    import torch
+    cat = _cat(81, n_gal=50)
+    g = catalog.Grid.square(100., 100)
+    s = torch.cuda.Stream()
+    ax = torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda")
+    ay = torch.empty_like(ax)
+    dcat = ctx.upload(cat)
+    ctx.gradient_grid(dcat, g, out=(ax, ay), stream=s)
+    ctx.synchronize(s)
+    ox, oy = oracle_lib.grad_grid(cat, g)
+    assert max_rel_err(ax.cpu().numpy(), ox) <= TOL
+    assert max_rel_err(ay.cpu().numpy(), oy) <= TOL
+
+
+def test_kmap_multi_plane_vs_oracle(ctx, oracle_lib):
+    cat = _cat(81, n_gal=90)
+    rng = np.random.default_rng(5)
+    cat.dlsds = np.repeat(rng.uniform(0.3, 0.9, 4), [2, 30, 30, 30])
+    g = catalog.Grid.square(80., 48)
+    m = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "mass"], kmap=True, mult=2.)
+    oh = oracle_lib.hess_grid(cat, g, kmap=True)
+    assert max_rel_err(m["hess_a"], oh[0]) <= TOL
+    assert max_rel_err(m["hess_b"], oh[1]) <= TOL
+    assert max_rel_err(m["hess_c"], oh[2]) <= TOL
+    assert max_rel_err(m["mass"], (oh[0] + oh[2]) * 0.5 * 2.) <= 1e-12
+
+
+def test_empty_and_single_halo(ctx, oracle_lib):
+    g = catalog.Grid.square(10., 16)
+    empty = _cat(81, n_gal=10).subset(np.array([], dtype=np.int64))
+    ax, ay = ctx.gradient_grid(empty, g)
+    assert not ax.any() and not ay.any()
+    m = ctx.hessian_maps(empty, g, ["mu", "kappa", "ampli3"], dlsds=0.5)
+    assert np.all(m["mu"] == 1.) and not m["kappa"].any() and not m["ampli3"].any()
+    one = _cat(81, n_gal=10).subset(np.array([3]))
+    ox, oy = oracle_lib.grad_grid(one, g)
+    ax, ay = ctx.gradient_grid(one, g)
+    assert max_rel_err(ax, ox) <= TOL and max_rel_err(ay, oy) <= TOL
+
+
+def test_errors_are_statuses(ctx):
+    g = catalog.Grid.square(10., 8)
+    bad = _cat(81, n_gal=10)
+    bad.type = bad.type.copy()
+    bad.type[4] = 14
+    with pytest.raises(lt.LensError) as e:
+        ctx.upload(bad)
+    assert e.value.status == 2
+    nan = _cat(81, n_gal=10)
+    nan.b0 = nan.b0.copy()
+    nan.b0[2] = np.nan
+    with pytest.raises(lt.LensError) as e:
+        ctx.upload(nan)
+    assert e.value.status == 3
+    cut = _cat(81, n_gal=10)
+    cut.rcut = cut.rcore.copy()
+    with pytest.raises(lt.LensError) as e:
+        ctx.upload(cut)
+    assert e.value.status == 3
+    with pytest.raises(lt.LensError) as e:
+        ctx.hessian_maps(_cat(81, n_gal=3), g, [99])
+    assert e.value.status == 1
+    small = lt.Context(0, budget_bytes=4096)
+    with pytest.raises(lt.LensError) as e:
+        small.upload(_cat(81, n_gal=500))
+    assert e.value.status == 6
+    small.close()
+
+
+def test_c1_scale_subsample_fp64(ctx, oracle_lib):
+    """1000 halos on the 4096^2 grid: the FP64 Hessian maps on a pixel subsample
+    (65536 seeded pixels plus every pixel within 3 rcore of a halo centre)."""
+    import torch
+    cat, g = catalog.workload("maps_1000h_4096")
+    D = 0.6
+    outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in ("kappa", "gamma1", "gamma2")}
+    ctx.hessian_maps(ctx.upload(cat), g, list(outs), dlsds=D, out=list(outs.values()))
+    ctx.synchronize()
+    rng = np.random.default_rng(20261204)
+    idx = rng.choice(g.npix, 65536, replace=False)
+    near = []
+    for x0, y0, rc in zip(cat.position_x, cat.position_y, cat.rcore):
+        i = int(round((x0 - g.xmin) / g.dx)); j = int(round((y0 - g.ymin) / g.dy))
+        r = int(np.ceil(3 * rc / g.dx)) + 1
+        for jj in range(max(0, j - r), min(g.ny, j + r + 1)):
+            for ii in range(max(0, i - r), min(g.nx, i + r + 1)):
+                near.append(jj * g.nx + ii)
+    idx = np.unique(np.concatenate([idx, np.array(near, np.int64)]))
+    px, py = g.coords(idx)
+    a, b, c, d = oracle_lib.hess_points(cat, px, py)
+    rms = {}
+    for k, ref in (("kappa", (a + c) * D / 2), ("gamma1", (a - c) * D / 2), ("gamma2", b * D)):
+        got = outs[k].cpu().numpy().ravel()[idx]
+        full = outs[k].cpu().numpy()
+        rms[k] = float(np.sqrt(np.mean(full * full)))
+        err = np.max(np.abs(got - ref) / np.maximum(np.abs(ref), rms[k]))
+        assert err <= TOL, (k, err)
