@@ -156,6 +156,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", type=int, default=0, help="smaller square grid (profiling cases)")
+    ap.add_argument("--maps", default="all", choices=["all", "hessian", "potential"],
+                    help="all = kappa/gamma1/gamma2/mu/psi (the workload); the others time one sum")
+    ap.add_argument("--breakdown", action="store_true", help="also time the Hessian-only and potential-only passes")
     args = ap.parse_args()
     warmup = max(args.warmup, 3)
     rank, local_rank, world = dist_env()
@@ -183,16 +187,20 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     build.build()
     cat, g = catalog.workload(WORKLOAD)
+    if args.grid:
+        g = catalog.Grid.square(150., args.grid)
     dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
     D = dls / dos
     ctx = lt.Context(local_rank)
     dcat = ctx.upload(cat)
     stream = torch.cuda.Stream()
-    names = ("kappa", "gamma1", "gamma2", "mu", "psi")
+    names = {"all": ("kappa", "gamma1", "gamma2", "mu", "psi"), "hessian": ("kappa", "gamma1", "gamma2", "mu"),
+             "potential": ("psi",)}[args.maps]
+    sums_per_pair = (2 if args.maps == "all" else 1)
     outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in names}
 
-    def step():
-        ctx.lens_maps(dcat, g, precision=args.precision, dlsds=D, out=outs, stream=stream)
+    def step(which=names, o=outs):
+        ctx.lens_maps(dcat, g, precision=args.precision, dlsds=D, out=o, stream=stream, which=which)
 
     for _ in range(warmup):
         step()
@@ -227,7 +235,23 @@ def main():
     if world > 1:
         dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
     elapsed = float(tmax.item())
-    evals_step = 2 * g.npix * cat.n
+    evals_step = sums_per_pair * g.npix * cat.n
+
+    breakdown = None
+    if args.breakdown and rank == 0:
+        breakdown = {}
+        for label, which in (("hessian_maps", ("kappa", "gamma1", "gamma2", "mu")), ("potential", ("psi",))):
+            o = {k: outs[k] for k in which}
+            step(which, o)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                step(which, o)
+            e1.record(stream)
+            ctx.synchronize(stream)
+            dt = e0.elapsed_time(e1) / 1e3 / args.steps
+            breakdown[label] = {"ms": dt * 1e3, "evals_per_s": g.npix * cat.n / dt}
     value = world * evals_step * args.steps / elapsed
 
     # end to end through the public API with host buffers: catalogue upload from host
@@ -238,13 +262,13 @@ def main():
         hnp = {k: v.numpy() for k, v in host.items()}
         for _ in range(1):
             c2 = ctx.upload(cat)
-            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp)
+            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp, which=names)
             c2.release()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             c2 = ctx.upload(cat)
-            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp)
+            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp, which=names)
             c2.release()
         torch.cuda.synchronize()
         te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
@@ -260,7 +284,8 @@ def main():
         peaks = measured_peaks()
         pipe = "fp64" if args.precision == "fp64" else "fp32"
         peak_tflops = fma_peak_tflops(pipe)
-        achieved = evals_step * FLOPS_PER_PAIR / 2 / per_launch / 1e12
+        fpp = {"all": FLOPS_PER_PAIR, "hessian": 182, "potential": 760}[args.maps]
+        achieved = g.npix * cat.n * fpp / per_launch / 1e12
         out_bytes = len(names) * g.npix * 8
         cpu = None
         if not args.no_cpu_baseline:
@@ -274,7 +299,8 @@ def main():
             "warmup": warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": f"{g.nx}x{g.ny} over 300\"x300\"", "halos": cat.n,
+            "config": {"workload": WORKLOAD if not args.grid else f"{WORKLOAD} at {g.nx}x{g.ny}",
+                       "grid": f"{g.nx}x{g.ny} over 300\"x300\"", "halos": cat.n,
                        "maps": list(names), "precision": args.precision, "evals_per_step": evals_step,
                        "parallelism": f"replicas x{world}",
                        "l2": "outputs 671 MB per step > 126 MB L2; catalogue 192 KB stays resident"},
@@ -283,7 +309,7 @@ def main():
                          "frac": achieved / peak_tflops if peak_tflops else None, "traffic": None,
                          "kernel": f"lt::grid64_kernel<OP_HESS|OP_POT>" if args.precision == "fp64" else
                          "lt::grid32c_kernel",
-                         "flops_per_pair": FLOPS_PER_PAIR, "flop_convention": "weighted census, FMA-equivalents",
+                         "flops_per_pair": fpp, "flop_convention": "weighted census, FMA-equivalents",
                          "peak_source": f"measured in-run: {pipe} FMA-chain kernel",
                          "hbm_writeback_gbs": out_bytes / per_launch / 1e9,
                          "hbm_peak_gbs": peaks.get("hbm_gbs")},
@@ -291,6 +317,8 @@ def main():
         }
         if e2e:
             line["e2e"] = e2e
+        if breakdown:
+            line["breakdown"] = breakdown
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line))

@@ -199,10 +199,21 @@ def test_c1_scale_subsample_fp64(ctx, oracle_lib):
     idx = np.unique(np.concatenate([idx, np.array(near, np.int64)]))
     px, py = g.coords(idx)
     a, b, c, d = oracle_lib.hess_points(cat, px, py)
-    rms = {}
-    for k, ref in (("kappa", (a + c) * D / 2), ("gamma1", (a - c) * D / 2), ("gamma2", b * D)):
+    # The reference formula is ill-conditioned within ~1e-3" of each halo's removable
+    # singular points (0, 2 r sqrt(eps)) of the halo frame: there a 1-ulp change of the
+    # pixel coordinate moves the reference's own result by up to ~1e-8.  Each pixel is
+    # held to 1e-12 plus 16x that measured 1-ulp sensitivity.
+    pert = [oracle_lib.hess_points(cat, np.nextafter(px, s * np.inf), py) for s in (1, -1)]
+    pert += [oracle_lib.hess_points(cat, px, np.nextafter(py, s * np.inf)) for s in (1, -1)]
+    for k, f in (("kappa", lambda h: (h[0] + h[2]) * D / 2), ("gamma1", lambda h: (h[0] - h[2]) * D / 2),
+                 ("gamma2", lambda h: h[1] * D)):
+        ref = f((a, b, c, d))
         got = outs[k].cpu().numpy().ravel()[idx]
         full = outs[k].cpu().numpy()
-        rms[k] = float(np.sqrt(np.mean(full * full)))
-        err = np.max(np.abs(got - ref) / np.maximum(np.abs(ref), rms[k]))
-        assert err <= TOL, (k, err)
+        rms = float(np.sqrt(np.mean(full * full)))
+        den = np.maximum(np.abs(ref), rms)
+        sens = np.max([np.abs(f(p) - ref) for p in pert], axis=0) / den
+        err = np.abs(got - ref) / den
+        assert np.all(err <= TOL + 16 * sens), (k, float(err.max()), float(sens[np.argmax(err)]))
+        # away from those points the plain bound holds
+        assert np.max(err[sens < 1e-14]) <= TOL, k
