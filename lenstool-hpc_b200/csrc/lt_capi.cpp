@@ -27,17 +27,6 @@ namespace lt {
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 } // namespace lt
 
-struct lt_catalog {
-    lt_rec64 *recs = nullptr;
-    lt_chunk *chunks = nullptr;
-    int32_t nhalos = 0;
-    int32_t nchunks = 0;
-    size_t bytes = 0;
-    std::vector<lt_rec64> host_recs; /* packed copy, reused by the FP32 packing */
-    void *aux = nullptr;             /* precision-specific device data */
-    size_t aux_bytes = 0;
-};
-
 /* ------------------------------------------------------------------ helpers ---- */
 
 void lt::set_error(lt_context *ctx, const char *fmt, ...)
@@ -90,6 +79,23 @@ lt_status lt::scratch_planes(lt_context *ctx, int n, size_t plane_bytes, double 
         ctx->scratch_bytes = need;
     }
     for (int i = 0; i < n; i++) planes[i] = (double *)((char *)ctx->scratch + (size_t)i * plane_bytes);
+    return LT_OK;
+}
+
+/* Pixel list (and its counter, in the first 16 bytes) of the recomputation pass. */
+lt_status lt::list_buffer(lt_context *ctx, long npix, int32_t **list, int32_t **count)
+{
+    size_t need = 16 + sizeof(int32_t) * (size_t)npix;
+    if (need > ctx->list_bytes) {
+        dev_free(ctx, ctx->list, ctx->list_bytes);
+        ctx->list = nullptr;
+        ctx->list_bytes = 0;
+        lt_status st = dev_alloc(ctx, &ctx->list, need);
+        if (st != LT_OK) return st;
+        ctx->list_bytes = need;
+    }
+    *count = (int32_t *)ctx->list;
+    *list = (int32_t *)((char *)ctx->list + 16);
     return LT_OK;
 }
 
@@ -269,6 +275,7 @@ lt_status lt_destroy(lt_context *ctx)
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     dev_free(ctx, ctx->scratch, ctx->scratch_bytes);
+    dev_free(ctx, ctx->list, ctx->list_bytes);
     dev_free(ctx, ctx->status, 64);
     destroy_extensions(ctx);
     delete ctx;
@@ -292,6 +299,7 @@ lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *s, lt_catalog **
     if (!cat) return LT_ERR_OUT_OF_MEMORY;
     cat->nhalos = s->nhalos;
     cat->host_recs.resize(s->nhalos);
+    cat->host_types.assign(s->type, s->type + s->nhalos);
     for (int i = 0; i < s->nhalos; i++) pack_one(s, i, cat->host_recs[i]);
     std::vector<lt_chunk> ch = make_chunks(s->type, s->nhalos, LT_CHUNK);
     cat->nchunks = (int32_t)ch.size();

@@ -31,9 +31,13 @@ struct GridArgs {
     double *out[LT_MAX_MAPS];
     double D, mult, scale;
     int32_t *status; /* device word: 0, or an lt_status set by a kernel */
+    /* list mode: evaluate the pixels list[0 .. min(*list_count, list_cap)) */
+    const int32_t *list;
+    const int32_t *list_count;
+    int32_t list_cap;
 };
 
 /* Launch the FP64 grid kernel for the sums in `op` (OP_* mask).  Returns the CUDA error. */
-int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream);
+int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode = false);
 
 } // namespace lt

@@ -1,18 +1,480 @@
 /*
- * lt_grid32.cu -- FP32-compensated grid path (placeholder until the kernel lands).
+ * lt_grid32.cu -- the FP32-compensated (LT_FP32C) Hessian-map path.
+ *
+ * Pass 1 (grid32c_kernel), per pixel tile:
+ *   - cluster-scale halos (b0 >= 5", rcore >= 1", or e < 1e-3) are summed in FP64 from
+ *     the FP64 records;
+ *   - every other halo is evaluated with the FP32 forms of lt_profiles32.cuh, unless any
+ *     pixel of the warp lies in one of the halo's FP64 regions (near the galaxy where
+ *     b0/2r > 0.1, within 0.3 rcut of the cut radius' singular point, within 3 rcore of
+ *     the centre); then the warp evaluates that halo in FP64 (warp-uniform branch);
+ *   - FP32 terms are rotated to the sky frame and added with Kahan compensation; the
+ *     pixel total combines the FP64 and compensated FP32 sums in FP64, and the Jacobian
+ *     determinant (1-k)^2 - g^2 is formed in FP64.
+ *   - pixels whose magnification exceeds the flag threshold (near critical curves, where
+ *     the determinant amplifies any error) are appended to a device list.
+ * Pass 2 (the FP64 grid kernel in list mode) recomputes the flagged pixels in FP64 and
+ * overwrites them.  The pixel count of pass 2 is read on the device: no host round trip.
  */
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "lt_bulk.cuh"
 #include "lt_internal.h"
+#include "lt_profiles32.cuh"
+#include "lt_profiles64.cuh"
 
 namespace lt {
 
-lt_status prepare_catalog_extensions(lt_context *, lt_catalog *) { return LT_OK; }
+/* FP32C catalogue: FP32 records + a chunk list over both record kinds
+ * (chunk.pad = 1: FP32 records of recs32, 0: FP64 records of recs64). */
+struct Fp32cCatalog {
+    lt_rec32 *recs32;
+    lt_chunk *chunks;
+    int32_t nchunks;
+    int32_t n32;
+};
 
-int launch_fp32c(lt_context *ctx, const lt_catalog *, int, GridArgs &, void *)
+static const double kTau = 0.1;        /* FP64 where b0 / (2 r) > kTau                */
+static const double kSingFrac = 0.3;   /* FP64 within 0.3 rcut of the singular point  */
+static const double kCoreFrac = 3.0;   /* FP64 within 3 rcore of the centre           */
+static const double kMuFlag = 4.0;     /* recompute pixels with |mu| above this       */
+
+static bool needs_fp64_always(const lt_rec64 &r, int type)
 {
-    set_error(ctx, "FP32C precision is not available in this build");
-    return (int)cudaErrorNotSupported;
+    if (r.b0 >= 5.0) return true;      /* cluster-scale halo */
+    if (type != 5 && r.rc >= 1.0) return true;
+    if (type != 5 && r.eps < 1e-3) return true; /* ci ~ 1/(2 sqrt(e)) amplification */
+    return false;
 }
 
-void destroy_extensions(lt_context *) {}
+static void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
+{
+    memset(&o, 0, sizeof(o));
+    o.x0 = r.x0;
+    o.y0 = r.y0;
+    o.cs = (float)r.cs;
+    o.sn = (float)r.sn;
+    o.c2t = (float)(r.cs * r.cs - r.sn * r.sn);
+    o.s2t = (float)(2. * r.cs * r.sn);
+    o.w = (float)r.w;
+    o.type = type;
+    o.idx64 = idx64;
+    const double e = r.eps;
+    const double near_r = r.b0 / (2. * kTau);
+    o.rnear2 = (float)(near_r * near_r);
+    if (type == 5) {
+        o.cx1 = (float)(1. - e);
+        o.icx1 = (float)(1. + e);
+        o.kpre = (float)(r.b0 * (1. - e) * (1. + e));
+        o.ppre = (float)r.b0;
+        o.singv = 0.f;
+        o.sing_r2 = 0.f;
+        o.core_r2 = 0.f;
+        return;
+    }
+    const double sqe = sqrt(e);
+    const double cx1 = (1. - e) / (1. + e);
+    const double ci = 0.5 * (1. - e * e) / sqe;
+    const double t05 = (type == 81) ? r.rcut / (r.rcut - r.rc) : 1.0;
+    o.s2 = (float)(2. * sqe);
+    o.cx1 = (float)cx1;
+    o.icx1 = (float)(1. / cx1);
+    o.cxi = (float)(1. / ((1. + e) * (1. + e)));
+    o.cyi = (float)(1. / ((1. - e) * (1. - e)));
+    o.ome2 = (float)(1. / (1. - e * e));
+    o.e4 = (float)(4. * e);
+    o.cpi = (float)(cx1 + 1. / cx1);
+    o.rc = (float)r.rc;
+    o.rcut = (float)r.rcut;
+    o.drs = (float)(r.rc - r.rcut);
+    o.dr2 = (float)((r.rc - r.rcut) * (r.rc + r.rcut));
+    o.rc2 = (float)(r.rc * r.rc);
+    o.rcut2 = (float)(r.rcut * r.rcut);
+    o.s2rc = (float)(2. * sqe * r.rc);
+    o.s2rcut = (float)(2. * sqe * r.rcut);
+    o.gpre = (float)(0.5 * ci * r.b0 * t05);
+    o.kpre = (float)(type == 81 ? -0.5 * r.b0 * t05 : 0.5 * r.b0);
+    o.ppre = (float)(ci * r.b0 * t05);
+    o.e1 = (float)(2. * sqe / (1. - e));
+    o.e2 = (float)(2. * sqe / (1. + e));
+    const double sr = type == 81 ? r.rcut : r.rc;
+    o.singv = (float)(2. * sr * sqe);
+    o.sing_r2 = (float)((kSingFrac * sr) * (kSingFrac * sr));
+    o.core_r2 = (float)((kCoreFrac * r.rc) * (kCoreFrac * r.rc));
+}
+
+lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
+{
+    const int n = cat->nhalos;
+    const std::vector<int32_t> &types = cat->host_types;
+    std::vector<lt_chunk> host_chunks;
+    /* FP64-class halos keep their FP64 records; the others get FP32 records.  Chunks
+     * never mix precision or type. */
+    std::vector<lt_rec32> r32;
+    std::vector<int32_t> t32;
+    std::vector<int32_t> idx64_always, t64;
+    for (int i = 0; i < n; i++) {
+        if (needs_fp64_always(cat->host_recs[i], types[i])) {
+            idx64_always.push_back(i);
+            t64.push_back(types[i]);
+        } else {
+            lt_rec32 o;
+            pack32(cat->host_recs[i], types[i], i, o);
+            r32.push_back(o);
+            t32.push_back(types[i]);
+        }
+    }
+    /* FP64-class chunks: runs of consecutive original indices of one type */
+    for (size_t k = 0; k < idx64_always.size();) {
+        size_t e = k + 1;
+        while (e < idx64_always.size() && idx64_always[e] == idx64_always[e - 1] + 1 && t64[e] == t64[k] &&
+               (int)(e - k) < LT_CHUNK)
+            e++;
+        lt_chunk c;
+        c.start = idx64_always[k];
+        c.count = (int32_t)(e - k);
+        c.type = t64[k];
+        c.pad = 0;
+        host_chunks.push_back(c);
+        k = e;
+    }
+    std::vector<lt_chunk> c32 = make_chunks(t32.data(), (int)t32.size(), LT_CHUNK);
+    for (lt_chunk c : c32) {
+        c.pad = 1;
+        host_chunks.push_back(c);
+    }
+    Fp32cCatalog h;
+    h.n32 = (int32_t)r32.size();
+    h.nchunks = (int32_t)host_chunks.size();
+    size_t rb = sizeof(lt_rec32) * r32.size(), cb = sizeof(lt_chunk) * host_chunks.size();
+    size_t total = sizeof(Fp32cCatalog) + rb + cb + 64;
+    void *mem = nullptr;
+    lt_status st = dev_alloc(ctx, &mem, total);
+    if (st != LT_OK) return st;
+    char *base = (char *)mem;
+    h.recs32 = (lt_rec32 *)(base + 64);
+    h.chunks = (lt_chunk *)(base + 64 + rb);
+    cudaError_t e = cudaSuccess;
+    if (rb) e = cudaMemcpy(h.recs32, r32.data(), rb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && cb) e = cudaMemcpy(h.chunks, host_chunks.data(), cb, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        dev_free(ctx, mem, total);
+        return cuda_fail(ctx, e, "FP32 catalogue upload");
+    }
+    /* the descriptor stays on the host side of the catalogue, the data on the device */
+    static_assert(sizeof(Fp32cCatalog) <= sizeof(((lt_catalog *)0)->aux_desc), "descriptor size");
+    cat->aux = mem;
+    cat->aux_bytes = total;
+    memcpy(cat->aux_desc, &h, sizeof(h));
+    return LT_OK;
+}
+
+constexpr int kThreads32 = 256;
+
+struct C32Args {
+    GridArgs g;
+    const lt_rec32 *recs32;
+    const lt_chunk *chunks; /* mixed list, pad = 1 for FP32 records */
+    int32_t nchunks;
+    int32_t *list;
+    int32_t *list_count;
+    int32_t list_cap;
+    double mu_flag;
+};
+
+template <int P>
+struct Acc32 {
+    double hxx[P], hyy[P], hxy[P], psi[P]; /* FP64 terms, sky frame */
+    float ks[P], kc[P], g1s[P], g1c[P], g2s[P], g2c[P], ps[P], pc[P]; /* Kahan sums of FP32 terms */
+};
+
+template <int OP, int P, int TYPE>
+__device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, const double (&px)[P], double py, int kmap,
+                                             Acc32<P> &acc)
+{
+#pragma unroll 1
+    for (int h = 0; h < count; h++) {
+        const lt_rec64 &r = recs[h];
+        const double w = kmap ? r.w : 1.0;
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            if (OP & OP_HESS) {
+                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
+                hess_pair<TYPE>(r, px[k], py, w, hh);
+                acc.hxx[k] = hh.xx;
+                acc.hyy[k] = hh.yy;
+                acc.hxy[k] = hh.xy;
+            }
+            if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
+        }
+    }
+}
+
+template <int OP, int P, int TYPE>
+__device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec64 *recs64, int count,
+                                             const double (&px)[P], double py, int kmap, Acc32<P> &acc)
+{
+#pragma unroll 1
+    for (int h = 0; h < count; h++) {
+        const lt_rec32 &r = recs[h];
+        float u[P], v[P];
+        bool near = false;
+        const float ty = (float)(py - r.y0);
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            const float tx = (float)(px[k] - r.x0);
+            u[k] = tx * r.cs + ty * r.sn;
+            v[k] = ty * r.cs - tx * r.sn;
+            const float rr = u[k] * u[k] + v[k] * v[k];
+            const float dv = v[k] - r.singv;
+            near |= (rr < r.rnear2) | (u[k] * u[k] + dv * dv < r.sing_r2) | (rr < r.core_r2);
+        }
+        if (OP & OP_POT) {
+#pragma unroll
+            for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
+        }
+        if (!(OP & OP_HESS)) continue;
+        if (__any_sync(0xffffffffu, near)) {
+            const lt_rec64 &r64 = recs64[r.idx64];
+            const double w = kmap ? r64.w : 1.0;
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
+                hess_pair<TYPE>(r64, px[k], py, w, hh);
+                acc.hxx[k] = hh.xx;
+                acc.hyy[k] = hh.yy;
+                acc.hxy[k] = hh.xy;
+            }
+        } else {
+            const float w = kmap ? r.w : 1.0f;
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                KG32 t = hess32<TYPE>(r, u[k], v[k]);
+                const float g1 = t.g1 * r.c2t - t.g2 * r.s2t;
+                const float g2 = t.g1 * r.s2t + t.g2 * r.c2t;
+                kahan_add(acc.ks[k], acc.kc[k], w * t.k);
+                kahan_add(acc.g1s[k], acc.g1c[k], w * g1);
+                kahan_add(acc.g2s[k], acc.g2c[k], w * g2);
+            }
+        }
+    }
+}
+
+template <int OP, int P>
+__global__ void __launch_bounds__(kThreads32, 1) grid32c_kernel(const C32Args A)
+{
+    const GridArgs &a = A.g;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[2];
+    unsigned char *buf0 = smem;
+    unsigned char *buf1 = smem + LT_CHUNK * sizeof(lt_rec64);
+
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    constexpr int kTileW = 32 * P;
+    const int ox = (warp & 3) * (8 * P) + (lane & 7) * P;
+    const int oy = (warp >> 2) * 4 + (lane >> 3);
+    const int my_tiles = (blockIdx.x < a.ntiles) ? (a.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const long steps = (long)my_tiles * A.nchunks;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (steps == 0) return;
+
+    auto issue = [&](long s) {
+        const lt_chunk c = A.chunks[s % A.nchunks];
+        unsigned char *dst = (s & 1) ? buf1 : buf0;
+        uint64_t *bar = &bars[s & 1];
+        const void *src;
+        uint32_t bytes;
+        if (c.pad) {
+            src = A.recs32 + c.start;
+            bytes = (uint32_t)c.count * (uint32_t)sizeof(lt_rec32);
+        } else {
+            src = a.recs + c.start;
+            bytes = (uint32_t)c.count * (uint32_t)sizeof(lt_rec64);
+        }
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_g2s(dst, src, bytes, bar);
+    };
+    if (tid == 0) issue(0);
+
+    uint32_t phase0 = 0, phase1 = 0;
+    Acc32<P> acc;
+    double px[P], py = 0.;
+    int ix = 0, iy = 0;
+
+    for (long s = 0; s < steps; s++) {
+        const int ci = (int)(s % A.nchunks);
+        if (ci == 0) {
+            const int tile = blockIdx.x + (int)(s / A.nchunks) * gridDim.x;
+            const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+            ix = tx * kTileW + ox;
+            iy = ty * 8 + oy;
+            py = pixel_y(a, iy < a.ny ? iy : a.ny - 1);
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                px[k] = pixel_x(a, (ix + k) < a.nx ? ix + k : a.nx - 1);
+                acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
+                acc.ks[k] = acc.kc[k] = acc.g1s[k] = acc.g1c[k] = acc.g2s[k] = acc.g2c[k] = 0.f;
+                acc.ps[k] = acc.pc[k] = 0.f;
+            }
+        }
+        if (tid == 0 && s + 1 < steps) issue(s + 1);
+        const int b = (int)(s & 1);
+        const uint32_t par = b ? phase1 : phase0;
+        if (!wait_tile(&bars[b], par, a.status)) {
+            if (tid == 0 && s + 1 < steps) drain_tile(&bars[b ^ 1], b ? phase0 : phase1);
+            return;
+        }
+        if (b) phase1 ^= 1; else phase0 ^= 1;
+
+        const lt_chunk c = A.chunks[ci];
+        const unsigned char *buf = b ? buf1 : buf0;
+        if (c.pad) {
+            const lt_rec32 *recs = reinterpret_cast<const lt_rec32 *>(buf);
+            switch (c.type) {
+            case 81: eval32_chunk<OP, P, 81>(recs, a.recs, c.count, px, py, a.kmap, acc); break;
+            case 8: eval32_chunk<OP, P, 8>(recs, a.recs, c.count, px, py, a.kmap, acc); break;
+            case 5: eval32_chunk<OP, P, 5>(recs, a.recs, c.count, px, py, a.kmap, acc); break;
+            default: break;
+            }
+        } else {
+            const lt_rec64 *recs = reinterpret_cast<const lt_rec64 *>(buf);
+            switch (c.type) {
+            case 81: eval64_chunk<OP, P, 81>(recs, c.count, px, py, a.kmap, acc); break;
+            case 8: eval64_chunk<OP, P, 8>(recs, c.count, px, py, a.kmap, acc); break;
+            case 5: eval64_chunk<OP, P, 5>(recs, c.count, px, py, a.kmap, acc); break;
+            default: break;
+            }
+        }
+
+        if (ci == A.nchunks - 1 && iy < a.ny) {
+            const long row = (long)iy * a.nx;
+            double hxx[P], hyy[P], hxy[P], psi[P];
+            bool flag[P];
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                const double kap = 0.5 * (acc.hxx[k] + acc.hyy[k]) + ((double)acc.ks[k] - (double)acc.kc[k]);
+                const double g1 = 0.5 * (acc.hxx[k] - acc.hyy[k]) + ((double)acc.g1s[k] - (double)acc.g1c[k]);
+                const double g2 = acc.hxy[k] + ((double)acc.g2s[k] - (double)acc.g2c[k]);
+                hxx[k] = kap + g1;
+                hyy[k] = kap - g1;
+                hxy[k] = g2;
+                psi[k] = acc.psi[k] + ((double)acc.ps[k] - (double)acc.pc[k]);
+                const double kd = kap * a.D, g1d = g1 * a.D, g2d = g2 * a.D;
+                const double det = (1. - kd) * (1. - kd) - g1d * g1d - g2d * g2d;
+                flag[k] = (OP & OP_HESS) && !(fabs(det) * A.mu_flag >= 1.0);
+            }
+            const bool full = a.vec_ok && (ix + P <= a.nx);
+            for (int o = 0; o < a.nout; o++) {
+                double v[P];
+#pragma unroll
+                for (int k = 0; k < P; k++)
+                    v[k] = map_value(a.kinds[o], 0., 0., hxx[k], hyy[k], hxy[k], psi[k], a.D, a.mult, a.scale);
+                double *dst = a.out[o] + row + ix;
+                if (P == 2 && full) {
+                    *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1 % P]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < P; k++)
+                        if (ix + k < a.nx) dst[k] = v[k];
+                }
+            }
+            if (A.list) {
+#pragma unroll
+                for (int k = 0; k < P; k++)
+                    if (flag[k] && ix + k < a.nx) {
+                        const int slot = atomicAdd(A.list_count, 1);
+                        if (slot < A.list_cap) A.list[slot] = (int32_t)(row + ix + k);
+                    }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+/* maps whose value depends on the Jacobian determinant (amplified near critical curves) */
+static bool det_sensitive(int kind)
+{
+    return kind == LT_MAP_MU || kind == LT_MAP_AMPLI1 || kind == LT_MAP_AMPLI2 || kind == LT_MAP_AMPLI3 ||
+           kind == LT_MAP_AMPLI4 || kind == LT_MAP_SHEAR2;
+}
+
+int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    const Fp32cCatalog &fc = *reinterpret_cast<const Fp32cCatalog *>(&cat->aux_desc);
+    if (op & OP_GRAD) {
+        set_error(ctx, "FP32C is implemented for the Hessian maps; use LT_FP64 for deflections");
+        return (int)cudaErrorNotSupported;
+    }
+    int err = cudaSuccess;
+    C32Args A;
+    memset(&A, 0, sizeof(A));
+    A.g = a;
+    bool det = false;
+    for (int o = 0; o < a.nout; o++) det |= det_sensitive(a.kinds[o]);
+    const int tile_w = 64, tile_h = 8;
+    A.g.tiles_x = (a.nx + tile_w - 1) / tile_w;
+    A.g.ntiles = A.g.tiles_x * ((a.ny + tile_h - 1) / tile_h);
+    A.recs32 = fc.recs32;
+    A.chunks = fc.chunks;
+    A.nchunks = fc.nchunks;
+    A.mu_flag = det ? kMuFlag : 0.0;
+    const long npix = (long)a.nx * a.ny;
+    if (det) {
+        lt_status st = list_buffer(ctx, npix, &A.list, &A.list_count);
+        if (st != LT_OK) return (int)cudaErrorMemoryAllocation;
+        A.list_cap = (int32_t)npix;
+        cudaMemsetAsync(A.list_count, 0, sizeof(int32_t), s);
+    }
+    const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
+    void (*kern)(const C32Args) = nullptr;
+    switch (op) {
+    case OP_HESS: kern = grid32c_kernel<OP_HESS, 2>; break;
+    case OP_POT: kern = grid32c_kernel<OP_POT, 2>; break;
+    case OP_HESS | OP_POT: kern = grid32c_kernel<OP_HESS | OP_POT, 2>; break;
+    default: return (int)cudaErrorInvalidValue;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads32, smem);
+    if (per_sm < 1) per_sm = 1;
+    int blocks = ctx->num_sms * per_sm;
+    if (blocks > A.g.ntiles) blocks = A.g.ntiles;
+    kern<<<blocks, kThreads32, smem, s>>>(A);
+    count_launch(1);
+    err = (int)cudaGetLastError();
+    if (err != cudaSuccess || !det) return err;
+    /* pass 2: FP64 recomputation of the flagged pixels' Hessian maps (the potential of
+     * those pixels keeps its FP32C value) */
+    GridArgs r = A.g;
+    r.nout = 0;
+    for (int o = 0; o < a.nout; o++)
+        if (a.kinds[o] != KIND_POT) {
+            r.kinds[r.nout] = a.kinds[o];
+            r.out[r.nout++] = a.out[o];
+        }
+    r.list = A.list;
+    r.list_count = A.list_count;
+    r.list_cap = A.list_cap;
+    err = launch_grid64_list(OP_HESS, r, ctx->num_sms, stream);
+    count_launch(1);
+    return err;
+}
+
+void destroy_extensions(lt_context *ctx)
+{
+    (void)ctx;
+}
 
 } // namespace lt

@@ -49,9 +49,10 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
     }
 }
 
-template <int OP, int P>
+template <int OP, int P, bool LIST>
 __global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
 {
+    static_assert(!LIST || P == 1, "list mode evaluates one pixel per thread");
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
     lt_rec64 *buf0 = reinterpret_cast<lt_rec64 *>(smem);
@@ -63,7 +64,13 @@ __global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
     const int ox = (warp & 3) * (8 * P) + (lane & 7) * P; /* pixel offset in the tile */
     const int oy = (warp >> 2) * 4 + (lane >> 3);
 
-    const int my_tiles = (blockIdx.x < a.ntiles) ? (a.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    int ntiles = a.ntiles, nlist = 0;
+    if (LIST) {
+        nlist = *a.list_count;
+        nlist = nlist < a.list_cap ? nlist : a.list_cap;
+        ntiles = (nlist + kThreads - 1) / kThreads;
+    }
+    const int my_tiles = ((int)blockIdx.x < ntiles) ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const long steps = (long)my_tiles * a.nchunks;
 
     if (tid == 0) {
@@ -94,9 +101,16 @@ __global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
         const int ci = (int)(s % a.nchunks);
         if (ci == 0) {
             const int tile = blockIdx.x + (int)(s / a.nchunks) * gridDim.x;
-            const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
-            ix = tx * kTileW + ox;
-            iy = ty * 8 + oy;
+            if (LIST) {
+                const int e = tile * kThreads + tid;
+                const int p = a.list[e < nlist ? e : nlist - 1];
+                ix = p % a.nx;
+                iy = e < nlist ? p / a.nx : a.ny; /* rows >= ny are not stored */
+            } else {
+                const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
+                ix = tx * kTileW + ox;
+                iy = ty * 8 + oy;
+            }
             const int cy = iy < a.ny ? iy : a.ny - 1;
             py = pixel_y(a, cy);
 #pragma unroll
@@ -149,11 +163,11 @@ __global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
     }
 }
 
-template <int OP, int P>
+template <int OP, int P, bool LIST = false>
 static int launch_op(const GridArgs &args, int num_sms, cudaStream_t stream)
 {
     const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
-    auto kern = grid64_kernel<OP, P>;
+    auto kern = grid64_kernel<OP, P, LIST>;
     static bool configured = false;
     if (!configured) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -163,15 +177,19 @@ static int launch_op(const GridArgs &args, int num_sms, cudaStream_t stream)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     int blocks = num_sms * per_sm;
-    if (blocks > args.ntiles) blocks = args.ntiles;
+    if (!LIST && blocks > args.ntiles) blocks = args.ntiles;
     if (blocks < 1) blocks = 1;
     kern<<<blocks, kThreads, smem, stream>>>(args);
     return (int)cudaGetLastError();
 }
 
-int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream)
+int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode)
 {
     cudaStream_t s = (cudaStream_t)stream;
+    if (list_mode) {
+        if (op != OP_HESS) return (int)cudaErrorInvalidValue;
+        return launch_op<OP_HESS, 1, true>(args, num_sms, s);
+    }
     switch (op) {
     case OP_GRAD: return launch_op<OP_GRAD, 2>(args, num_sms, s);
     case OP_HESS: return launch_op<OP_HESS, 2>(args, num_sms, s);
@@ -184,6 +202,12 @@ int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream)
 } // namespace lt
 
 namespace lt {
+
+int launch_grid64_list(int op, GridArgs &a, int num_sms, void *stream)
+{
+    a.vec_ok = 0;
+    return launch_grid64(op, a, num_sms, stream, true);
+}
 
 /* Maps of an empty catalogue: the epilogue evaluated on zero sums. */
 __global__ void epilogue_zero_kernel(const GridArgs a)

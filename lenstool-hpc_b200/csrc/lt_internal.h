@@ -22,6 +22,21 @@ struct lt_context {
     size_t scratch_bytes = 0;
     int32_t *status = nullptr; /* device status word written by kernels */
     void *ext = nullptr;       /* state of the batch and serving extensions */
+    void *list = nullptr;      /* pixel list of the FP32C recomputation pass (+ count) */
+    size_t list_bytes = 0;
+};
+
+struct lt_catalog {
+    lt_rec64 *recs = nullptr;            /* FP64 records, device */
+    lt_chunk *chunks = nullptr;          /* FP64 chunk list, device */
+    int32_t nhalos = 0;
+    int32_t nchunks = 0;
+    size_t bytes = 0;
+    std::vector<lt_rec64> host_recs;     /* packed records, host copy */
+    std::vector<int32_t> host_types;     /* profile type per halo */
+    void *aux = nullptr;                 /* FP32C records and chunks, device */
+    size_t aux_bytes = 0;
+    alignas(16) unsigned char aux_desc[64]; /* FP32C descriptor (host) */
 };
 
 namespace lt {
@@ -39,6 +54,8 @@ lt_status run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g, int
                    double mult, double scale, int nout, const int *kinds, double *const *outs, void *stream);
 int launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream);
 int launch_epilogue_zero(const GridArgs &a, int num_sms, void *stream);
+int launch_grid64_list(int op, GridArgs &a, int num_sms, void *stream);
+lt_status list_buffer(lt_context *ctx, long npix, int32_t **list, int32_t **count);
 
 /* FP32-compensated path (lt_grid32.cu) */
 lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat);

@@ -3,4 +3,4 @@
 TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and bench.py's
 cpu_baseline / reference legs; never by the product package.
 """
-from .oracle import Oracle, RefLib, ORACLE_SO, REF_SO, build  # noqa: F401
+from .oracle import Oracle, RefLib, ORACLE_SO, ORACLE_LD_SO, REF_SO, build  # noqa: F401

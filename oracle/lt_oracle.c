@@ -23,6 +23,16 @@
 #include <omp.h>
 #endif
 
+/* LTO_EXTENDED builds the same arithmetic in x87 extended precision (64-bit mantissa),
+ * liblt_oracle_ld.so: the difference between the two builds measures the FP64 rounding
+ * error of the reference's own formulas at each pixel. */
+#ifdef LTO_EXTENDED
+#include <tgmath.h>
+typedef long double real;
+#else
+typedef double real;
+#endif
+
 typedef struct {
     int n;
     const int *type;
@@ -48,84 +58,88 @@ enum { LTO_OK = 0, LTO_ERR_PROFILE = 2, LTO_ERR_ARG = 1 };
 /* SIS deflection of halo i, src/gradient.cpp:260-299 (the _v2 variant).  The inverse
  * radius starts from a single-precision square root followed by one Newton step
  * (src/gradient.cpp:287-288). */
-static void sis_grad_acc(const lto_cat *c, int i, double px, double py, double *gx, double *gy)
+static void sis_grad_acc(const lto_cat *c, int i, real px, real py, real *gx, real *gy)
 {
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double b0 = c->b0[i];
-    double cs = c->cs[i], sn = c->sn[i];
-    double u = tx * cs + ty * sn;
-    double v = ty * cs - tx * sn;
-    double e = c->eps[i];
-    double q = u * u * (1. - e) + v * v * (1. + e);
-    double r = 1. / sqrtf((float)q);
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real b0 = c->b0[i];
+    real cs = c->cs[i], sn = c->sn[i];
+    real u = tx * cs + ty * sn;
+    real v = ty * cs - tx * sn;
+    real e = c->eps[i];
+    real q = u * u * (1. - e) + v * v * (1. + e);
+#ifdef LTO_EXTENDED
+    real r = 1. / sqrt(q); /* the exact inverse radius the seed approximates */
+#else
+    real r = 1. / sqrtf((float)q);
     r = r * (1.5 - 0.5 * q * r * r);
-    double fx = (1. - e) * b0 * u * r;
-    double fy = (1. + e) * b0 * v * r;
+#endif
+    real fx = (1. - e) * b0 * u * r;
+    real fy = (1. + e) * b0 * v * r;
     *gx += fx * cs - fy * sn;
     *gy += fy * cs + fx * sn;
 }
 
 /* One complex-logarithm term of the PIEMD deflection for core radius r: the KERNEL
  * macro of src/gradient.hpp:64-76 (also piemd_1derivatives_ci05, src/gradient.cpp:60-100). */
-static void piemd_term(double u, double v, double r, double sqe, double cx1, double rem2,
-                       double zci_im, double *re, double *im)
+static void piemd_term(real u, real v, real r, real sqe, real cx1, real rem2,
+                       real zci_im, real *re, real *im)
 {
-    double nre = cx1 * u;
-    double nim = 2. * sqe * sqrt(r * r + rem2) - v / cx1;
-    double dim = 2. * r * sqe - v;
-    double nrm = (u * u + dim * dim);
-    double zre = (nre * u + nim * dim) / nrm;
-    double zim = (nim * u - nre * dim) / nrm;
-    double m = zre;
-    double lre = log(sqrt(m * m + zim * zim));
-    double lim = atan2(zim, m);
+    real nre = cx1 * u;
+    real nim = 2. * sqe * sqrt(r * r + rem2) - v / cx1;
+    real dim = 2. * r * sqe - v;
+    real nrm = (u * u + dim * dim);
+    real zre = (nre * u + nim * dim) / nrm;
+    real zim = (nim * u - nre * dim) / nrm;
+    real m = zre;
+    real lre = log(sqrt(m * m + zim * zim));
+    real lim = atan2(zim, m);
     *re = -zci_im * lim;
     *im = zci_im * lre;
 }
 
 /* PIEMD deflection, src/gradient.cpp:548-607. */
-static void piemd_grad_acc(const lto_cat *c, int i, double px, double py, double *gx, double *gy)
+static void piemd_grad_acc(const lto_cat *c, int i, real px, real py, real *gx, real *gy)
 {
-    double b0 = c->b0[i];
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double cs = c->cs[i], sn = c->sn[i];
-    double u = tx * cs + ty * sn;
-    double v = ty * cs - tx * sn;
-    double e = c->eps[i];
-    double rc = c->rc[i];
-    double sqe = sqrt(e);
-    double cx1 = (1. - e) / (1. + e);
-    double cxro = (1. + e) * (1. + e);
-    double cyro = (1. - e) * (1. - e);
-    double rem2 = u * u / cxro + v * v / cyro;
-    double zci_im = -0.5 * (1. - e * e) / sqe;
-    double re, im;
+    real b0 = c->b0[i];
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real cs = c->cs[i], sn = c->sn[i];
+    real u = tx * cs + ty * sn;
+    real v = ty * cs - tx * sn;
+    real e = c->eps[i];
+    real rc = c->rc[i];
+    real sqe = sqrt(e);
+    real cx1 = (1. - e) / (1. + e);
+    real cxro = (1. + e) * (1. + e);
+    real cyro = (1. - e) * (1. - e);
+    real rem2 = u * u / cxro + v * v / cyro;
+    real zci_im = -0.5 * (1. - e * e) / sqe;
+    real re, im;
     piemd_term(u, v, rc, sqe, cx1, rem2, zci_im, &re, &im);
     *gx += b0 * (re * cs - im * sn);
     *gy += b0 * (im * cs + re * sn);
 }
 
 /* Cut dPIE deflection, src/gradient.cpp:744-811: t05 * (K(rcore) - K(rcut)). */
-static void dpie_grad_acc(const lto_cat *c, int i, double px, double py, double *gx, double *gy)
+static void dpie_grad_acc(const lto_cat *c, int i, real px, real py, real *gx, real *gy)
 {
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double cs = c->cs[i], sn = c->sn[i];
-    double u = tx * cs + ty * sn;
-    double v = ty * cs - tx * sn;
-    double e = c->eps[i];
-    double rc = c->rc[i], rcut = c->rcut[i], b0 = c->b0[i];
-    double t05 = b0 * rcut / (rcut - rc);
-    double sqe = sqrt(e);
-    double cx1 = (1. - e) / (1. + e);
-    double cxro = (1. + e) * (1. + e);
-    double cyro = (1. - e) * (1. - e);
-    double rem2 = u * u / cxro + v * v / cyro;
-    double zci_im = -0.5 * (1. - e * e) / sqe;
-    double are, aim, bre, bim;
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real cs = c->cs[i], sn = c->sn[i];
+    real u = tx * cs + ty * sn;
+    real v = ty * cs - tx * sn;
+    real e = c->eps[i];
+    real rc = c->rc[i], rcut = c->rcut[i], b0 = c->b0[i];
+    real t05 = b0 * rcut / (rcut - rc);
+    real sqe = sqrt(e);
+    real cx1 = (1. - e) / (1. + e);
+    real cxro = (1. + e) * (1. + e);
+    real cyro = (1. - e) * (1. - e);
+    real rem2 = u * u / cxro + v * v / cyro;
+    real zci_im = -0.5 * (1. - e * e) / sqe;
+    real are, aim, bre, bim;
     piemd_term(u, v, rc, sqe, cx1, rem2, zci_im, &are, &aim);
     piemd_term(u, v, rcut, sqe, cx1, rem2, zci_im, &bre, &bim);
-    double zre = t05 * (are - bre);
-    double zim = t05 * (aim - bim);
+    real zre = t05 * (are - bre);
+    real zim = t05 * (aim - bim);
     *gx += (zre * cs - zim * sn);
     *gy += (zim * cs + zre * sn);
 }
@@ -133,15 +147,15 @@ static void dpie_grad_acc(const lto_cat *c, int i, double px, double py, double 
 /* Sum over halos at one point, dispatched over runs of equal type:
  * module_potentialDerivatives_totalGradient_SOA, src/gradient.cpp:899-929.  Each run is
  * summed on its own and then added to the total, as the reference does. */
-static int grad_point(const lto_cat *c, double px, double py, double *ax, double *ay)
+static int grad_point(const lto_cat *c, real px, real py, double *ax, double *ay)
 {
-    double tx = 0., ty = 0.;
+    real tx = 0., ty = 0.;
     int s = 0;
     while (s < c->n) {
         int t = c->type[s];
         int e = s + 1;
         while (e < c->n && c->type[e] == t) e++;
-        double rx = 0., ry = 0.;
+        real rx = 0., ry = 0.;
         switch (t) {
         case 5:  for (int i = s; i < e; i++) sis_grad_acc(c, i, px, py, &rx, &ry); break;
         case 8:  for (int i = s; i < e; i++) piemd_grad_acc(c, i, px, py, &rx, &ry); break;
@@ -161,26 +175,26 @@ static int grad_point(const lto_cat *c, double px, double py, double *ax, double
 /* Hessian                                                                            */
 /* ---------------------------------------------------------------------------------- */
 
-typedef struct { double a, b, c, d; } lto_mat;
+typedef struct { real a, b, c, d; } lto_mat;
 
 /* Second derivatives of one PIEMD term I0.5 (Kassiola & Kovner 1993):
  * mdci05_hpc, src/gradient2.cpp:54-83. */
-static lto_mat mdci05(double x, double y, double eps, double rc, double b0)
+static lto_mat mdci05(real x, real y, real eps, real rc, real b0)
 {
-    double sqe = sqrt(eps);
-    double cx1 = (1. - eps) / (1. + eps);
-    double cx1inv = 1. / cx1;
-    double cxro = (1. + eps) * (1. + eps);
-    double cyro = (1. - eps) * (1. - eps);
-    double ci = 0.5 * (1. - eps * eps) / sqe;
-    double wrem = sqrt(rc * rc + x * x / cxro + y * y / cyro);
-    double den1 = 2. * sqe * wrem - y * cx1inv;
+    real sqe = sqrt(eps);
+    real cx1 = (1. - eps) / (1. + eps);
+    real cx1inv = 1. / cx1;
+    real cxro = (1. + eps) * (1. + eps);
+    real cyro = (1. - eps) * (1. - eps);
+    real ci = 0.5 * (1. - eps * eps) / sqe;
+    real wrem = sqrt(rc * rc + x * x / cxro + y * y / cyro);
+    real den1 = 2. * sqe * wrem - y * cx1inv;
     den1 = cx1 * cx1 * x * x + den1 * den1;
-    double num2 = 2. * rc * sqe - y;
-    double den2 = x * x + num2 * num2;
-    double didxre = ci * (cx1 * (2. * sqe * x * x / cxro / wrem - 2. * sqe * wrem + y * cx1inv) / den1 + num2 / den2);
-    double didyre = ci * ((2. * sqe * x * y * cx1 / cyro / wrem - x) / den1 + x / den2);
-    double didyim = ci * ((2. * sqe * wrem * cx1inv - y * cx1inv * cx1inv - 4. * eps * y / cyro +
+    real num2 = 2. * rc * sqe - y;
+    real den2 = x * x + num2 * num2;
+    real didxre = ci * (cx1 * (2. * sqe * x * x / cxro / wrem - 2. * sqe * wrem + y * cx1inv) / den1 + num2 / den2);
+    real didyre = ci * ((2. * sqe * x * y * cx1 / cyro / wrem - x) / den1 + x / den2);
+    real didyim = ci * ((2. * sqe * wrem * cx1inv - y * cx1inv * cx1inv - 4. * eps * y / cyro +
                            2. * sqe * y * y / cyro / wrem * cx1inv) / den1 - num2 / den2);
     lto_mat r;
     r.a = b0 * didxre;
@@ -191,7 +205,7 @@ static lto_mat mdci05(double x, double y, double eps, double rc, double b0)
 
 /* Rotate a Hessian from the halo frame back to the sky frame, H = R^T H' R, with the
  * two-step order of src/gradient2.cpp:146-156. */
-static void rotate_back_acc(lto_mat h, double cs, double sn, lto_mat *acc)
+static void rotate_back_acc(lto_mat h, real cs, real sn, lto_mat *acc)
 {
     lto_mat m;
     m.a = h.a * cs + h.b * -sn;
@@ -205,13 +219,13 @@ static void rotate_back_acc(lto_mat h, double cs, double sn, lto_mat *acc)
 }
 
 /* dPIE Hessian, src/gradient2.cpp:92-205 (elliptical branch, taken for every halo). */
-static void dpie_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat *acc)
+static void dpie_hess_acc(const lto_cat *c, int i, real px, real py, lto_mat *acc)
 {
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double cs = c->cs[i], sn = c->sn[i];
-    double u = tx * cs + ty * sn;
-    double v = ty * cs - tx * sn;
-    double t05 = c->rcut[i] / (c->rcut[i] - c->rc[i]);
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real cs = c->cs[i], sn = c->sn[i];
+    real u = tx * cs + ty * sn;
+    real v = ty * cs - tx * sn;
+    real t05 = c->rcut[i] / (c->rcut[i] - c->rc[i]);
     lto_mat core = mdci05(u, v, c->eps[i], c->rc[i], c->b0[i]);
     lto_mat cut = mdci05(u, v, c->eps[i], c->rcut[i], c->b0[i]);
     core.a = t05 * (core.a - cut.a);
@@ -223,12 +237,12 @@ static void dpie_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat
 
 /* PIEMD Hessian (restated; the reference has no type-8 Hessian): one mdci05 term with
  * impact parameter b0, the dPIE structure of src/gradient2.cpp:92-156 without the cut. */
-static void piemd_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat *acc)
+static void piemd_hess_acc(const lto_cat *c, int i, real px, real py, lto_mat *acc)
 {
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double cs = c->cs[i], sn = c->sn[i];
-    double u = tx * cs + ty * sn;
-    double v = ty * cs - tx * sn;
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real cs = c->cs[i], sn = c->sn[i];
+    real u = tx * cs + ty * sn;
+    real v = ty * cs - tx * sn;
     lto_mat h = mdci05(u, v, c->eps[i], c->rc[i], c->b0[i]);
     rotate_back_acc(h, cs, sn, acc);
 }
@@ -237,16 +251,16 @@ static void piemd_hess_acc(const lto_cat *c, int i, double px, double py, lto_ma
  * With R^2 = (1-e)u^2 + (1+e)v^2 in the halo frame:
  *   psi_uu = b0 (1-e)(1+e) v^2 / R^3,  psi_vv = b0 (1-e)(1+e) u^2 / R^3,
  *   psi_uv = -b0 (1-e)(1+e) u v / R^3. */
-static void sis_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat *acc)
+static void sis_hess_acc(const lto_cat *c, int i, real px, real py, lto_mat *acc)
 {
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double cs = c->cs[i], sn = c->sn[i];
-    double u = tx * cs + ty * sn;
-    double v = ty * cs - tx * sn;
-    double e = c->eps[i];
-    double q = u * u * (1. - e) + v * v * (1. + e);
-    double r = sqrt(q);
-    double k = c->b0[i] * (1. - e) * (1. + e) / (q * r);
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real cs = c->cs[i], sn = c->sn[i];
+    real u = tx * cs + ty * sn;
+    real v = ty * cs - tx * sn;
+    real e = c->eps[i];
+    real q = u * u * (1. - e) + v * v * (1. + e);
+    real r = sqrt(q);
+    real k = c->b0[i] * (1. - e) * (1. + e) / (q * r);
     lto_mat h;
     h.a = k * v * v;
     h.c = k * u * u;
@@ -258,13 +272,13 @@ static void sis_hess_acc(const lto_cat *c, int i, double px, double py, lto_mat 
  * (src/gradient2.cpp:226-254).  With kmap != 0 the runs also break where dlsds changes
  * and each run is weighted by its dlsds: module_potentialDerivatives_Kmap_SOA_GPU,
  * src/gradient2_GPU.cu:455-522. */
-static int hess_point(const lto_cat *c, double px, double py, int kmap, lto_mat *out)
+static int hess_point(const lto_cat *c, real px, real py, int kmap, lto_mat *out)
 {
     lto_mat tot = {0., 0., 0., 0.};
     int s = 0;
     while (s < c->n) {
         int t = c->type[s];
-        double w = kmap ? c->dlsds[s] : 1.;
+        real w = kmap ? c->dlsds[s] : 1.;
         int e = s + 1;
         while (e < c->n && c->type[e] == t && (!kmap || c->dlsds[e] == w)) e++;
         lto_mat r = {0., 0., 0., 0.};
@@ -289,7 +303,7 @@ static int hess_point(const lto_cat *c, double px, double py, int kmap, lto_mat 
 /* potential                                                                          */
 /* ---------------------------------------------------------------------------------- */
 
-typedef struct { double re, im; } lto_cpx;
+typedef struct { real re, im; } lto_cpx;
 
 static lto_cpx cx_add(lto_cpx a, lto_cpx b) { lto_cpx r = {a.re + b.re, a.im + b.im}; return r; }
 static lto_cpx cx_sub(lto_cpx a, lto_cpx b) { lto_cpx r = {a.re - b.re, a.im - b.im}; return r; }
@@ -298,12 +312,12 @@ static lto_cpx cx_mul(lto_cpx a, lto_cpx b)
     lto_cpx r = {a.re * b.re - a.im * b.im, a.im * b.re + b.im * a.re};
     return r;
 }
-static lto_cpx cx_scale(lto_cpx a, double f) { lto_cpx r = {a.re * f, a.im * f}; return r; }
+static lto_cpx cx_scale(lto_cpx a, real f) { lto_cpx r = {a.re * f, a.im * f}; return r; }
 static lto_cpx cx_sq(lto_cpx a) { lto_cpx r = {a.re * a.re - a.im * a.im, 2. * a.re * a.im}; return r; }
 /* a/b, zero when |b| = 0 (dcpx_GPU, src/lt_math_GPU.cuh:224-243). */
 static lto_cpx cx_div(lto_cpx a, lto_cpx b)
 {
-    double n = b.re * b.re + b.im * b.im;
+    real n = b.re * b.re + b.im * b.im;
     lto_cpx r = {0., 0.};
     if (n != 0.) {
         r.re = (a.re * b.re + a.im * b.im) / n;
@@ -313,13 +327,13 @@ static lto_cpx cx_div(lto_cpx a, lto_cpx b)
 }
 static lto_cpx cx_cosh(lto_cpx a)
 {
-    double ep = exp(a.re), em = exp(-a.re);
+    real ep = exp(a.re), em = exp(-a.re);
     lto_cpx r = {0.5 * (ep + em) * cos(a.im), 0.5 * (ep - em) * sin(a.im)};
     return r;
 }
 static lto_cpx cx_sinh(lto_cpx a)
 {
-    double ep = exp(a.re), em = exp(-a.re);
+    real ep = exp(a.re), em = exp(-a.re);
     lto_cpx r = {0.5 * (ep - em) * cos(a.im), 0.5 * (ep + em) * sin(a.im)};
     return r;
 }
@@ -331,16 +345,16 @@ static lto_cpx cx_log(lto_cpx a)
 
 /* Potential of one PIEMD term I0.5 at (x, y) in the halo frame: pi05_gpu,
  * src/potential_GPU.cu:47-72, with the complex helpers of src/lt_math_GPU.cuh. */
-static double pi05(double x, double y, double eps, double rc, double b0)
+static real pi05(real x, real y, real eps, real rc, real b0)
 {
-    double sqe = sqrt(eps);
-    double ci = .5 * (1. - eps * eps) / sqe;
-    double cxro = (1. + eps) * (1. + eps);
-    double cyro = (1. - eps) * (1. - eps);
-    double rem2 = x * x / cxro + y * y / cyro;
-    double e1 = 2. * sqe / (1 - eps);
-    double e2 = 2. * sqe / (1 + eps);
-    double z = sqrt(x * x + y * y);
+    real sqe = sqrt(eps);
+    real ci = .5 * (1. - eps * eps) / sqe;
+    real cxro = (1. + eps) * (1. + eps);
+    real cyro = (1. - eps) * (1. - eps);
+    real rem2 = x * x / cxro + y * y / cyro;
+    real e1 = 2. * sqe / (1 - eps);
+    real e2 = 2. * sqe / (1 + eps);
+    real z = sqrt(x * x + y * y);
     lto_cpx eta = {-.5 * asinh(e1 * y / z), .5 * asin(e2 * x / z)};
     lto_cpx zeta = {0.5 * log((sqrt(rem2) + sqrt(rc * rc + rem2)) / rc), 0.};
     lto_cpx b1 = cx_cosh(cx_add(eta, zeta));
@@ -353,10 +367,10 @@ static double pi05(double x, double y, double eps, double rc, double b0)
     return b0 * ci * rc / sqrt(rem2) * (ckk.im * x - ckk.re * y);
 }
 
-static void halo_frame(const lto_cat *c, int i, double px, double py, double *u, double *v)
+static void halo_frame(const lto_cat *c, int i, real px, real py, real *u, real *v)
 {
-    double tx = px - c->x[i], ty = py - c->y[i];
-    double cs = c->cs[i], sn = c->sn[i];
+    real tx = px - c->x[i], ty = py - c->y[i];
+    real cs = c->cs[i], sn = c->sn[i];
     *u = tx * cs + ty * sn;
     *v = ty * cs - tx * sn;
 }
@@ -364,27 +378,27 @@ static void halo_frame(const lto_cat *c, int i, double px, double py, double *u,
 /* Potential at one point: module_potential_totalPotential_SOA_GPU and
  * module_potential_81_SOA_GPU, src/potential_GPU.cu:75-187 (dPIE); SIS (b0 R) and
  * PIEMD (one pi05 term) are restated. */
-static int pot_point(const lto_cat *c, double px, double py, double *out)
+static int pot_point(const lto_cat *c, real px, real py, double *out)
 {
-    double tot = 0.;
+    real tot = 0.;
     int s = 0;
     while (s < c->n) {
         int t = c->type[s];
         int e = s + 1;
         while (e < c->n && c->type[e] == t) e++;
-        double r = 0.;
+        real r = 0.;
         for (int i = s; i < e; i++) {
-            double u, v;
+            real u, v;
             halo_frame(c, i, px, py, &u, &v);
             if (t == 81) {
-                double t05 = c->rcut[i] / (c->rcut[i] - c->rc[i]);
-                double pa = pi05(u, v, c->eps[i], c->rc[i], c->b0[i]);
-                double ps = pi05(u, v, c->eps[i], c->rcut[i], c->b0[i]);
+                real t05 = c->rcut[i] / (c->rcut[i] - c->rc[i]);
+                real pa = pi05(u, v, c->eps[i], c->rc[i], c->b0[i]);
+                real ps = pi05(u, v, c->eps[i], c->rcut[i], c->b0[i]);
                 r += t05 * (pa - ps);
             } else if (t == 8) {
                 r += pi05(u, v, c->eps[i], c->rc[i], c->b0[i]);
             } else if (t == 5) {
-                double e_ = c->eps[i];
+                real e_ = c->eps[i];
                 r += c->b0[i] * sqrt(u * u * (1. - e_) + v * v * (1. + e_));
             } else {
                 return LTO_ERR_PROFILE;
@@ -403,7 +417,7 @@ static int pot_point(const lto_cat *c, double px, double py, double *out)
 
 /* Pixel (ii, jj) sits at xmin + (ii + istart) dx, ymin + (jj + jstart) dy and is stored
  * at jj*nx + ii: gradient_grid_general_CPU, src/grid_gradient_CPU.cpp:67-100. */
-static void pixel_xy(const lto_grid *g, long p, double *px, double *py)
+static void pixel_xy(const lto_grid *g, long p, real *px, real *py)
 {
     int ii = (int)(p % g->nx), jj = (int)(p / g->nx);
     *px = g->xmin + (ii + g->istart) * g->dx;
@@ -426,7 +440,7 @@ int lto_grad_grid(const lto_cat *c, const lto_grid *g, double *ax, double *ay, i
     set_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
     for (long p = 0; p < np; p++) {
-        double px, py;
+        real px, py;
         pixel_xy(g, p, &px, &py);
         bad |= grad_point(c, px, py, &ax[p], &ay[p]);
     }
@@ -442,7 +456,7 @@ int lto_hess_grid(const lto_cat *c, const lto_grid *g, int kmap, double *a, doub
     set_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
     for (long p = 0; p < np; p++) {
-        double px, py;
+        real px, py;
         lto_mat m;
         pixel_xy(g, p, &px, &py);
         bad |= hess_point(c, px, py, kmap, &m);
@@ -458,7 +472,7 @@ int lto_pot_grid(const lto_cat *c, const lto_grid *g, double *psi, int nthreads)
     set_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 64) reduction(| : bad)
     for (long p = 0; p < np; p++) {
-        double px, py;
+        real px, py;
         pixel_xy(g, p, &px, &py);
         bad |= pot_point(c, px, py, &psi[p]);
     }
@@ -507,10 +521,10 @@ int lto_pot_points(const lto_cat *c, long np, const double *px, const double *py
 
 /* Eigenvalues of the symmetric 2x2 matrix [[a, b], [b, c]]: formeli_ampli,
  * src/grid_map_ampli_GPU.cu:549-572 (the orientation is not used by any map). */
-static void eigen2(double a, double b, double c, double *lam, double *mu)
+static void eigen2(real a, real b, real c, real *lam, real *mu)
 {
-    double delta = (a - c) * (a - c) + 4 * b * b;
-    double e = sqrt(delta);
+    real delta = (a - c) * (a - c) + 4 * b * b;
+    real e = sqrt(delta);
     *lam = .5 * (a + c + e);
     *mu = .5 * (a + c - e);
 }
@@ -531,32 +545,32 @@ int lto_map(int kind, long np, const double *a, const double *b, const double *c
             double scale, double *out)
 {
     for (long p = 0; p < np; p++) {
-        double A = 1. - a[p] * D, B = -b[p] * D, C = 1. - c[p] * D;
-        double lam, mu, r;
+        real A = 1. - a[p] * D, B = -b[p] * D, C = 1. - c[p] * D;
+        real lam, mu, r;
         switch (kind) {
         case LTO_MAP_AMPLI1: eigen2(A, B, C, &lam, &mu); r = 1. / (lam * mu); break;
         case LTO_MAP_AMPLI2: eigen2(A, B, C, &lam, &mu); r = 1. / fabs(lam * mu); break;
         case LTO_MAP_AMPLI3: eigen2(A, B, C, &lam, &mu); r = -2.5 * log10(fabs(lam * mu)); break;
         case LTO_MAP_AMPLI4: {
-            double k = (a[p] + c[p]) * D / 2.;
-            double g1 = (a[p] - c[p]) * D / 2.;
-            double g2 = b[p] * D;
-            double g = sqrt(g1 * g1 + g2 * g2);
-            double gp = g / (1 - k);
+            real k = (a[p] + c[p]) * D / 2.;
+            real g1 = (a[p] - c[p]) * D / 2.;
+            real g2 = b[p] * D;
+            real g = sqrt(g1 * g1 + g2 * g2);
+            real gp = g / (1 - k);
             r = (1 - k) * (1 + gp * gp) / (1 - gp * gp);
             break;
         }
         case LTO_MAP_AMPLI5: r = (a[p] + c[p]) / 2.; break;
         case LTO_MAP_AMPLI6: {
-            double g1 = (a[p] - c[p]) / 2.;
-            double g2 = b[p];
+            real g1 = (a[p] - c[p]) / 2.;
+            real g2 = b[p];
             r = sqrt(g1 * g1 + g2 * g2);
             break;
         }
         case LTO_MAP_SHEAR1: eigen2(A, B, C, &lam, &mu); r = (lam - mu) / 2.; break;
         case LTO_MAP_SHEAR2: {
             eigen2(A, B, C, &lam, &mu);
-            double q = lam / mu;
+            real q = lam / mu;
             r = fabs((q * q - 1.) / (q * q + 1.));
             break;
         }
@@ -566,9 +580,9 @@ int lto_map(int kind, long np, const double *a, const double *b, const double *c
         case LTO_MAP_GAMMA1: r = (a[p] - c[p]) * D / 2.; break;
         case LTO_MAP_GAMMA2: r = b[p] * D; break;
         case LTO_MAP_MU: {
-            double k = (a[p] + c[p]) * D / 2.;
-            double g1 = (a[p] - c[p]) * D / 2.;
-            double g2 = b[p] * D;
+            real k = (a[p] + c[p]) * D / 2.;
+            real g1 = (a[p] - c[p]) * D / 2.;
+            real g2 = b[p] * D;
             r = 1. / ((1. - k) * (1. - k) - g1 * g1 - g2 * g2);
             break;
         }

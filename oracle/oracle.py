@@ -19,6 +19,7 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liblt_oracle.so"
+ORACLE_LD_SO = HERE / "liblt_oracle_ld.so"
 REF_SO = HERE / "_ref" / "libltref.so"
 REFERENCE_TREE = pathlib.Path("/root/reference")
 

@@ -1,0 +1,101 @@
+"""FP32-compensated maps against the FP64 path (itself pinned to the oracle by
+test_gpu_parity.py).
+
+Bound: per pixel |fp32c - fp64| <= 1e-6 * max(|fp64|, RMS(fp64 map)), pixels with
+|mu| > 100 excluded (they are reported separately), as the accuracy target of the
+compensated path states."""
+import numpy as np
+import pytest
+
+import lenstool_hpc_b200 as lt
+from lenstool_hpc_b200 import catalog
+
+pytestmark = pytest.mark.gpu
+TOL32 = 1e-6
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lenstool_hpc_b200 import build
+    build.build()
+    c = lt.Context(0)
+    yield c
+    c.close()
+
+
+def rel_errors(got, ref, mask):
+    g = got[mask]
+    r = ref[mask]
+    rms = np.sqrt(np.mean(r * r))
+    e = np.abs(g - r) / np.maximum(np.abs(r), rms)
+    return float(e.max())
+
+
+def _maps(ctx, cat, g, precision, D=0.6, kinds=("kappa", "gamma1", "gamma2", "mu")):
+    import torch
+    outs = [torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for _ in kinds]
+    ctx.hessian_maps(cat, g, list(kinds), precision=precision, dlsds=D, out=outs)
+    ctx.synchronize()
+    return {k: o.cpu().numpy() for k, o in zip(kinds, outs)}
+
+
+def test_fp32c_workload_maps(ctx):
+    """The 1000-halo 4096^2 workload: kappa, gamma1, gamma2, mu within 1e-6."""
+    cat, g = catalog.workload("maps_1000h_4096")
+    dcat = ctx.upload(cat)
+    m64 = _maps(ctx, dcat, g, "fp64")
+    m32 = _maps(ctx, dcat, g, "fp32c")
+    mask = np.isfinite(m64["mu"]) & (np.abs(m64["mu"]) <= 100)
+    errs = {k: rel_errors(m32[k], m64[k], mask) for k in m64}
+    high = ~mask & np.isfinite(m64["mu"])
+    errs_high = {k: rel_errors(m32[k], m64[k], high) for k in ("kappa", "gamma1", "gamma2")} if high.any() else {}
+    print("fp32c max rel err (|mu|<=100):", errs, " |mu|>100 pixels:", int(high.sum()), errs_high)
+    for k, e in errs.items():
+        assert e <= TOL32, (k, e)
+
+
+@pytest.mark.parametrize("cluster_type", [81, 8, 5])
+def test_fp32c_mixed_profiles(ctx, cluster_type):
+    cat = catalog.cluster_galaxy_catalog(2, 150, 99, cluster_type=cluster_type)
+    g = catalog.Grid.square(100., 512)
+    m64 = _maps(ctx, cat, g, "fp64", kinds=("kappa", "gamma1", "gamma2", "mu", "ampli3", "shear2"))
+    m32 = _maps(ctx, cat, g, "fp32c", kinds=("kappa", "gamma1", "gamma2", "mu", "ampli3", "shear2"))
+    mask = np.isfinite(m64["mu"]) & (np.abs(m64["mu"]) <= 100)
+    for k in m64:
+        assert rel_errors(m32[k], m64[k], mask) <= TOL32, k
+
+
+def test_fp32c_sis_galaxies_and_kmap(ctx):
+    rng = np.random.default_rng(4)
+    n = 120
+    t = np.where(np.arange(n) < 60, 5, 81)
+    cat = catalog.make_catalog(t, rng.uniform(-60, 60, n), rng.uniform(-60, 60, n),
+                               np.exp(rng.uniform(np.log(80), np.log(300), n)), rng.uniform(0, 0.5, n),
+                               rng.uniform(0, np.pi, n), rng.uniform(0.05, 0.2, n), rng.uniform(5, 50, n))
+    cat.dlsds = np.where(np.arange(n) < 40, 0.5, 0.8)
+    g = catalog.Grid.square(80., 384)
+    import torch
+    o64 = [torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for _ in range(3)]
+    o32 = [torch.empty_like(o64[0]) for _ in range(3)]
+    kinds = ["hess_a", "hess_b", "mass"]
+    ctx.hessian_maps(cat, g, kinds, precision="fp64", kmap=True, mult=1.7, out=o64)
+    ctx.hessian_maps(cat, g, kinds, precision="fp32c", kmap=True, mult=1.7, out=o32)
+    ctx.synchronize()
+    mask = np.ones((g.ny, g.nx), bool)
+    for a, b, k in zip(o32, o64, kinds):
+        assert rel_errors(a.cpu().numpy(), b.cpu().numpy(), mask) <= TOL32, k
+
+
+def test_fp32c_host_outputs_and_potential(ctx):
+    """lens_maps in FP32C through host buffers; the potential stays FP64-exact."""
+    cat = catalog.cluster_galaxy_catalog(2, 80, 7)
+    g = catalog.Grid.square(100., 200)
+    a = ctx.lens_maps(cat, g, precision="fp32c", dlsds=0.6)
+    b = ctx.lens_maps(cat, g, precision="fp64", dlsds=0.6)
+    mask = np.isfinite(b["mu"]) & (np.abs(b["mu"]) <= 100)
+    for k in ("kappa", "gamma1", "gamma2", "mu"):
+        assert rel_errors(a[k], b[k], mask) <= TOL32, k
+    assert rel_errors(a["psi"], b["psi"], np.ones_like(mask)) <= 1e-6

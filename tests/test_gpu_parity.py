@@ -201,10 +201,14 @@ def test_c1_scale_subsample_fp64(ctx, oracle_lib):
     a, b, c, d = oracle_lib.hess_points(cat, px, py)
     # The reference formula is ill-conditioned within ~1e-3" of each halo's removable
     # singular points (0, 2 r sqrt(eps)) of the halo frame: there a 1-ulp change of the
-    # pixel coordinate moves the reference's own result by up to ~1e-8.  Each pixel is
-    # held to 1e-12 plus 16x that measured 1-ulp sensitivity.
+    # pixel coordinate moves the reference's own result by up to ~1e-8, and its FP64
+    # rounding error (measured against the extended-precision build of the oracle)
+    # grows alike.  Each pixel is held to 1e-12 plus 16x the larger of the two.
+    import oracle
+    ext = oracle.Oracle(oracle.ORACLE_LD_SO).hess_points(cat, px, py)
     pert = [oracle_lib.hess_points(cat, np.nextafter(px, s * np.inf), py) for s in (1, -1)]
     pert += [oracle_lib.hess_points(cat, px, np.nextafter(py, s * np.inf)) for s in (1, -1)]
+    pert.append(ext)
     for k, f in (("kappa", lambda h: (h[0] + h[2]) * D / 2), ("gamma1", lambda h: (h[0] - h[2]) * D / 2),
                  ("gamma2", lambda h: h[1] * D)):
         ref = f((a, b, c, d))
@@ -217,3 +221,4 @@ def test_c1_scale_subsample_fp64(ctx, oracle_lib):
         assert np.all(err <= TOL + 16 * sens), (k, float(err.max()), float(sens[np.argmax(err)]))
         # away from those points the plain bound holds
         assert np.max(err[sens < 1e-14]) <= TOL, k
+        print(k, "max err", float(err.max()), "pixels above 1e-12:", int((err > TOL).sum()))
