@@ -15,6 +15,7 @@
  */
 #include <cuda_runtime.h>
 #include "lt_bulk.cuh"
+#include "lt_internal.h"
 #include "lt_profiles64.cuh"
 
 namespace lt {
@@ -215,6 +216,21 @@ __global__ void epilogue_zero_kernel(const GridArgs a)
     const long npix = (long)a.nx * a.ny;
     for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x)
         for (int o = 0; o < a.nout; o++) a.out[o][p] = map_value(a.kinds[o], 0., 0., 0., 0., 0., 0., a.D, a.mult, a.scale);
+}
+
+__global__ void planes_epilogue_kernel(int kind, double *out, const double *a, const double *b, const double *c,
+                                       double D, double mult, long npix)
+{
+    for (long p = blockIdx.x * (long)blockDim.x + threadIdx.x; p < npix; p += (long)gridDim.x * blockDim.x)
+        out[p] = map_value(kind, 0., 0., a[p], c[p], b[p], a[p], D, mult, mult);
+}
+
+int launch_planes_epilogue(int kind, double *out, const double *a, const double *b, const double *c, double D,
+                           double mult, int nx, int ny, int num_sms, void *stream)
+{
+    planes_epilogue_kernel<<<num_sms * 4, 256, 0, (cudaStream_t)stream>>>(kind, out, a, b, c, D, mult, (long)nx * ny);
+    count_launch(1);
+    return (int)cudaGetLastError();
 }
 
 int launch_epilogue_zero(const GridArgs &a, int num_sms, void *stream)

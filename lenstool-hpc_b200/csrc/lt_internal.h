@@ -55,6 +55,9 @@ lt_status run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g, int
 int launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream);
 int launch_epilogue_zero(const GridArgs &a, int num_sms, void *stream);
 int launch_grid64_list(int op, GridArgs &a, int num_sms, void *stream);
+/* map kind `kind` of device planes a (xx), b (xy), c (yy) into `out` (in place allowed) */
+int launch_planes_epilogue(int kind, double *out, const double *a, const double *b, const double *c, double D,
+                           double mult, int nx, int ny, int num_sms, void *stream);
 lt_status list_buffer(lt_context *ctx, long npix, int32_t **list, int32_t **count);
 
 /* FP32-compensated path (lt_grid32.cu) */

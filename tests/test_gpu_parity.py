@@ -218,7 +218,8 @@ def test_c1_scale_subsample_fp64(ctx, oracle_lib):
         den = np.maximum(np.abs(ref), rms)
         sens = np.max([np.abs(f(p) - ref) for p in pert], axis=0) / den
         err = np.abs(got - ref) / den
-        assert np.all(err <= TOL + 16 * sens), (k, float(err.max()), float(sens[np.argmax(err)]))
+        bad = np.flatnonzero(err > TOL + 16 * sens)
+        assert bad.size == 0, (k, [(float(err[i]), float(sens[i]), float(px[i]), float(py[i])) for i in bad[:5]])
         # away from those points the plain bound holds
         assert np.max(err[sens < 1e-14]) <= TOL, k
         print(k, "max err", float(err.max()), "pixels above 1e-12:", int((err > TOL).sum()))
