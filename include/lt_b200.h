@@ -150,6 +150,20 @@ lt_status lt_lens_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *gr
                        double dlsds, double *kappa, double *gamma1, double *gamma2, double *mu, double *psi,
                        void *stream);
 
+/* ---- kernel shapes and the autotuner ----------------------------------------------
+ * A grid kernel comes in shapes: pixels per thread (1 or 2) and the resident CTAs per SM
+ * its register budget is cut for (1 or 2).  `sums` is a mask: 1 deflection, 2 Hessian,
+ * 4 potential (6 = the fused lens maps).  No counterpart in the reference (its launch
+ * shape is fixed, src/grid_gradient2_GPU.cu:28-29). */
+lt_status lt_set_kernel_shape(lt_context *ctx, int32_t precision, int32_t sums, int32_t pixels_per_thread,
+                              int32_t ctas_per_sm);
+lt_status lt_get_kernel_shape(const lt_context *ctx, int32_t precision, int32_t sums, int32_t *pixels_per_thread,
+                              int32_t *ctas_per_sm);
+/* Time every shape for (precision, sums) on a grid_n x grid_n grid covering the
+ * catalogue and keep the fastest in the context; *best_ms (may be NULL) gets its time. */
+lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision, int32_t sums, int32_t grid_n,
+                      double *best_ms);
+
 /* Wait for the context's work on `stream` and report any status a kernel recorded
  * (e.g. LT_ERR_TIMEOUT from a bounded device-side wait).  Asynchronous (device-pointer)
  * calls report such errors here. */

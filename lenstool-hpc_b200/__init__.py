@@ -78,7 +78,9 @@ _LIB = None
 # every symbol the C ABI exports (include/lt_b200.h)
 EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release", "lt_catalog_nhalos",
            "lt_gradient_grid", "lt_hessian_maps", "lt_potential_grid", "lt_lens_maps", "lt_synchronize",
-           "lt_cosmo_distances", "lt_kernel_launch_count", "lt_status_string", "lt_last_error", "lt_abi_version")
+           "lt_cosmo_distances", "lt_kernel_launch_count", "lt_status_string", "lt_last_error", "lt_abi_version",
+           "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_autotune", "lt_measure_fma_peak")
+SUMS = {"deflection": 1, "hessian": 2, "potential": 4, "lens": 6}
 
 
 def load_library(path=None):
@@ -103,6 +105,11 @@ def load_library(path=None):
     L.lt_lens_maps.argtypes = [vp, vp, C.POINTER(_Grid), C.c_int32, C.c_double, vp, vp, vp, vp, vp, vp]
     L.lt_synchronize.argtypes = [vp, vp]
     L.lt_cosmo_distances.argtypes = [C.POINTER(_Cosmo), C.c_double, C.c_double, _dp, _dp, _dp]
+    L.lt_set_kernel_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
+    L.lt_get_kernel_shape.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.lt_autotune.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+    L.lt_measure_fma_peak.argtypes = [C.c_int, C.c_int]
+    L.lt_measure_fma_peak.restype = C.c_double
     L.lt_kernel_launch_count.restype = C.c_uint64
     L.lt_status_string.restype = C.c_char_p
     L.lt_status_string.argtypes = [C.c_int]
@@ -266,6 +273,28 @@ class Context:
                                     *ptrs, _stream_handle(stream))
         self._check(st, "lt_lens_maps")
         return out
+
+    def set_kernel_shape(self, precision, sums, pixels_per_thread, ctas_per_sm):
+        st = self._lib.lt_set_kernel_shape(self.handle, PRECISION[precision], SUMS.get(sums, sums), pixels_per_thread,
+                                           ctas_per_sm)
+        self._check(st, "lt_set_kernel_shape")
+
+    def kernel_shape(self, precision, sums):
+        a, b = C.c_int32(), C.c_int32()
+        st = self._lib.lt_get_kernel_shape(self.handle, PRECISION[precision], SUMS.get(sums, sums), C.byref(a),
+                                           C.byref(b))
+        self._check(st, "lt_get_kernel_shape")
+        return a.value, b.value
+
+    def autotune(self, cat, precision="fp32c", sums="lens", grid_n=512):
+        """Time every kernel shape on a grid_n^2 grid over the catalogue; keep the fastest.
+        Returns (pixels_per_thread, ctas_per_sm, ms)."""
+        cat = self._cat(cat)
+        ms = C.c_double()
+        st = self._lib.lt_autotune(self.handle, cat.handle, PRECISION[precision], SUMS.get(sums, sums), grid_n,
+                                   C.byref(ms))
+        self._check(st, "lt_autotune")
+        return self.kernel_shape(precision, sums) + (ms.value,)
 
     def synchronize(self, stream=None):
         self._check(self._lib.lt_synchronize(self.handle, _stream_handle(stream)), "lt_synchronize")

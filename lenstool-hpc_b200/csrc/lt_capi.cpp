@@ -254,6 +254,14 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
     if (!ctx) return LT_ERR_OUT_OF_MEMORY;
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
+    /* default kernel shapes (pixels per thread, CTAs per SM); lt_autotune refines them */
+    for (int p = 0; p < 2; p++)
+        for (int o = 0; o < 8; o++) ctx->shape[p][o] = LT_SHAPE(2, 1);
+    ctx->shape[LT_FP64][OP_POT] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP64][OP_HESS | OP_POT] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP32C][OP_HESS] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP32C][OP_HESS | OP_POT] = LT_SHAPE(2, 2);
     cudaSetDevice(device);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -429,7 +437,7 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
             count_launch(1);
         }
     } else if (precision == LT_FP64) {
-        err = launch_grid64_tiled(op, a, ctx->num_sms, s);
+        err = launch_grid64_tiled(op, a, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
     } else {
         err = launch_fp32c(ctx, cat, op, a, s);
     }
@@ -445,12 +453,9 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
 }
 
 /* Tile bookkeeping shared by the launchers. */
-int lt::launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream)
+int lt::launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream, int shape)
 {
-    const int tile_w = 64, tile_h = 8;
-    a.tiles_x = (a.nx + tile_w - 1) / tile_w;
-    a.ntiles = a.tiles_x * ((a.ny + tile_h - 1) / tile_h);
-    int err = launch_grid64(op, a, num_sms, stream);
+    int err = launch_grid64(op, a, num_sms, stream, false, shape);
     count_launch(1);
     return err;
 }
@@ -524,6 +529,104 @@ lt_status lt_lens_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *gr
         return LT_ERR_INVALID_ARGUMENT;
     }
     return run_grid(ctx, cat, grid, precision, op, 0, dlsds, 1.0, dlsds, n, kinds, outs, stream);
+}
+
+} // extern "C"
+
+/* ------------------------------------------------------- shapes and autotuning ---- */
+
+static bool sums_ok(int precision, int sums)
+{
+    if (precision != LT_FP64 && precision != LT_FP32C) return false;
+    if (precision == LT_FP64) return sums == OP_GRAD || sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
+    return sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
+}
+
+extern "C" {
+
+lt_status lt_set_kernel_shape(lt_context *ctx, int32_t precision, int32_t sums, int32_t ppt, int32_t cps)
+{
+    if (!ctx || !sums_ok(precision, sums) || (ppt != 1 && ppt != 2) || (cps != 1 && cps != 2))
+        return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->shape[precision][sums] = LT_SHAPE(ppt, cps);
+    return LT_OK;
+}
+
+lt_status lt_get_kernel_shape(const lt_context *ctx, int32_t precision, int32_t sums, int32_t *ppt, int32_t *cps)
+{
+    if (!ctx || !ppt || !cps || !sums_ok(precision, sums)) return LT_ERR_INVALID_ARGUMENT;
+    const int s = ctx->shape[precision][sums];
+    *ppt = s & 15;
+    *cps = s >> 4;
+    return LT_OK;
+}
+
+lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision, int32_t sums, int32_t grid_n,
+                      double *best_ms)
+{
+    if (!ctx || !cat || !sums_ok(precision, sums) || grid_n < 8 || grid_n > 8192) return LT_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    /* a grid over the catalogue's extent (10% margin) */
+    double lo = -1., hi = 1.;
+    for (const lt_rec64 &r : cat->host_recs) {
+        lo = std::fmin(lo, std::fmin(r.x0, r.y0));
+        hi = std::fmax(hi, std::fmax(r.x0, r.y0));
+    }
+    const double pad = 0.1 * (hi - lo);
+    lt_grid g;
+    g.xmin = g.ymin = lo - pad;
+    g.dx = g.dy = (hi - lo + 2 * pad) / (grid_n - 1);
+    g.nx = g.ny = grid_n;
+    g.istart = g.jstart = 0;
+    int kinds[2];
+    int nout = 0;
+    if (sums & OP_GRAD) {
+        kinds[nout++] = KIND_GRAD_X;
+        kinds[nout++] = KIND_GRAD_Y;
+    }
+    if (sums & OP_HESS) kinds[nout++] = LT_MAP_KAPPA;
+    if (sums & OP_POT) kinds[nout++] = KIND_POT;
+    double *planes = nullptr;
+    const size_t plane = sizeof(double) * (size_t)grid_n * grid_n;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        lt_status st = dev_alloc(ctx, (void **)&planes, nout * plane);
+        if (st != LT_OK) return st;
+    }
+    double *outs[2] = {planes, planes + (size_t)grid_n * grid_n};
+    const int shapes[4] = {LT_SHAPE(1, 1), LT_SHAPE(1, 2), LT_SHAPE(2, 1), LT_SHAPE(2, 2)};
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 1e300;
+    int best_shape = ctx->shape[precision][sums];
+    lt_status st = LT_OK;
+    for (int k = 0; k < 4 && st == LT_OK; k++) {
+        ctx->shape[precision][sums] = shapes[k];
+        st = run_grid(ctx, cat, &g, precision, sums, 0, 1.0, 1.0, 1.0, nout, kinds, outs, nullptr);
+        if (st != LT_OK) break;
+        cudaEventRecord(e0, nullptr);
+        for (int rep = 0; rep < 2 && st == LT_OK; rep++)
+            st = run_grid(ctx, cat, &g, precision, sums, 0, 1.0, 1.0, 1.0, nout, kinds, outs, nullptr);
+        cudaEventRecord(e1, nullptr);
+        if (st == LT_OK) st = lt_synchronize(ctx, nullptr);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (st == LT_OK && ms / 2 < best) {
+            best = ms / 2;
+            best_shape = shapes[k];
+        }
+    }
+    ctx->shape[precision][sums] = best_shape;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        dev_free(ctx, planes, nout * plane);
+    }
+    if (best_ms) *best_ms = best;
+    return st;
 }
 
 } // extern "C"

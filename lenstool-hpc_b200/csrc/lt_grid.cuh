@@ -37,7 +37,12 @@ struct GridArgs {
     int32_t list_cap;
 };
 
+/* Kernel shape: pixels per thread (1 or 2) and resident CTAs per SM the register budget
+ * is cut for (1 or 2). */
+#define LT_SHAPE(ppt, cps) ((ppt) | ((cps) << 4))
+
 /* Launch the FP64 grid kernel for the sums in `op` (OP_* mask).  Returns the CUDA error. */
-int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode = false);
+int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode = false,
+                  int shape = LT_SHAPE(2, 1));
 
 } // namespace lt

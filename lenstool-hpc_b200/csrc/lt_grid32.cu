@@ -6,7 +6,7 @@
  *     the FP64 records;
  *   - every other halo is evaluated with the FP32 forms of lt_profiles32.cuh, unless any
  *     pixel of the warp lies in one of the halo's FP64 regions (near the galaxy where
- *     b0/2r > 0.1, within 0.3 rcut of the cut radius' singular point, within 3 rcore of
+ *     b0/2r > 0.1, within (0.3 + 1.5 e) rcut of the cut radius' singular point, within 3 rcore of
  *     the centre); then the warp evaluates that halo in FP64 (warp-uniform branch);
  *   - FP32 terms are rotated to the sky frame and added with Kahan compensation; the
  *     pixel total combines the FP64 and compensated FP32 sums in FP64, and the Jacobian
@@ -39,7 +39,10 @@ struct Fp32cCatalog {
 };
 
 static const double kTau = 0.1;        /* FP64 where b0 / (2 r) > kTau                */
-static const double kSingFrac = 0.3;   /* FP64 within 0.3 rcut of the singular point  */
+/* FP64 within (kSingFrac + kSingEps e) rcut of the singular point: the FP32 forms lose
+ * accuracy near it, more so at larger ellipticity */
+static const double kSingFrac = 0.3;
+static const double kSingEps = 1.5;
 static const double kCoreFrac = 3.0;   /* FP64 within 3 rcore of the centre           */
 static const double kMuFlag = 4.0;     /* recompute pixels with |mu| above this       */
 
@@ -103,7 +106,8 @@ static void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     o.e2 = (float)(2. * sqe / (1. + e));
     const double sr = type == 81 ? r.rcut : r.rc;
     o.singv = (float)(2. * sr * sqe);
-    o.sing_r2 = (float)((kSingFrac * sr) * (kSingFrac * sr));
+    const double srad = (kSingFrac + kSingEps * e) * sr;
+    o.sing_r2 = (float)(srad * srad);
     o.core_r2 = (float)((kCoreFrac * r.rc) * (kCoreFrac * r.rc));
 }
 
@@ -264,8 +268,8 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
     }
 }
 
-template <int OP, int P>
-__global__ void __launch_bounds__(kThreads32, 1) grid32c_kernel(const C32Args A)
+template <int OP, int P, int MINB>
+__global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args A)
 {
     const GridArgs &a = A.g;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -403,6 +407,27 @@ __global__ void __launch_bounds__(kThreads32, 1) grid32c_kernel(const C32Args A)
     }
 }
 
+template <int OP>
+static void (*pick_shape32(int shape))(const C32Args)
+{
+    switch (shape) {
+    case LT_SHAPE(1, 1): return grid32c_kernel<OP, 1, 1>;
+    case LT_SHAPE(1, 2): return grid32c_kernel<OP, 1, 2>;
+    case LT_SHAPE(2, 2): return grid32c_kernel<OP, 2, 2>;
+    default: return grid32c_kernel<OP, 2, 1>;
+    }
+}
+
+static void (*pick_kernel32(int op, int shape))(const C32Args)
+{
+    switch (op) {
+    case OP_HESS: return pick_shape32<OP_HESS>(shape);
+    case OP_POT: return pick_shape32<OP_POT>(shape);
+    case OP_HESS | OP_POT: return pick_shape32<OP_HESS | OP_POT>(shape);
+    default: return nullptr;
+    }
+}
+
 /* maps whose value depends on the Jacobian determinant (amplified near critical curves) */
 static bool det_sensitive(int kind)
 {
@@ -424,9 +449,10 @@ int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, vo
     A.g = a;
     bool det = false;
     for (int o = 0; o < a.nout; o++) det |= det_sensitive(a.kinds[o]);
-    const int tile_w = 64, tile_h = 8;
-    A.g.tiles_x = (a.nx + tile_w - 1) / tile_w;
-    A.g.ntiles = A.g.tiles_x * ((a.ny + tile_h - 1) / tile_h);
+    const int shape = ctx->shape[LT_FP32C][op & 7];
+    const int ppt = (shape & 15) == 1 ? 1 : 2;
+    A.g.tiles_x = (a.nx + 32 * ppt - 1) / (32 * ppt);
+    A.g.ntiles = A.g.tiles_x * ((a.ny + 7) / 8);
     A.recs32 = fc.recs32;
     A.chunks = fc.chunks;
     A.nchunks = fc.nchunks;
@@ -439,13 +465,8 @@ int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, vo
         cudaMemsetAsync(A.list_count, 0, sizeof(int32_t), s);
     }
     const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
-    void (*kern)(const C32Args) = nullptr;
-    switch (op) {
-    case OP_HESS: kern = grid32c_kernel<OP_HESS, 2>; break;
-    case OP_POT: kern = grid32c_kernel<OP_POT, 2>; break;
-    case OP_HESS | OP_POT: kern = grid32c_kernel<OP_HESS | OP_POT, 2>; break;
-    default: return (int)cudaErrorInvalidValue;
-    }
+    void (*kern)(const C32Args) = pick_kernel32(op, shape);
+    if (!kern) return (int)cudaErrorInvalidValue;
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads32, smem);
     if (per_sm < 1) per_sm = 1;

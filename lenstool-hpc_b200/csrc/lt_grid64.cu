@@ -50,8 +50,8 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
     }
 }
 
-template <int OP, int P, bool LIST>
-__global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
+template <int OP, int P, bool LIST, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a)
 {
     static_assert(!LIST || P == 1, "list mode evaluates one pixel per thread");
     extern __shared__ __align__(16) unsigned char smem[];
@@ -164,38 +164,49 @@ __global__ void __launch_bounds__(kThreads, 1) grid64_kernel(const GridArgs a)
     }
 }
 
-template <int OP, int P, bool LIST = false>
+/* Launch one shape: P pixels per thread, registers cut for MINB resident CTAs per SM.
+ * Tiles are (32 P) x 8 pixels; persistent grid of (resident CTAs per SM) x SMs. */
+template <int OP, int P, bool LIST, int MINB>
 static int launch_op(const GridArgs &args, int num_sms, cudaStream_t stream)
 {
     const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
-    auto kern = grid64_kernel<OP, P, LIST>;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = true;
-    }
+    auto kern = grid64_kernel<OP, P, LIST, MINB>;
+    GridArgs a = args;
+    a.tiles_x = (a.nx + 32 * P - 1) / (32 * P);
+    a.ntiles = a.tiles_x * ((a.ny + 7) / 8);
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
     if (per_sm < 1) per_sm = 1;
     int blocks = num_sms * per_sm;
-    if (!LIST && blocks > args.ntiles) blocks = args.ntiles;
+    if (!LIST && blocks > a.ntiles) blocks = a.ntiles;
     if (blocks < 1) blocks = 1;
-    kern<<<blocks, kThreads, smem, stream>>>(args);
+    kern<<<blocks, kThreads, smem, stream>>>(a);
     return (int)cudaGetLastError();
 }
 
-int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode)
+template <int OP>
+static int launch_shape(int shape, const GridArgs &a, int num_sms, cudaStream_t s)
+{
+    switch (shape) {
+    case LT_SHAPE(1, 1): return launch_op<OP, 1, false, 1>(a, num_sms, s);
+    case LT_SHAPE(1, 2): return launch_op<OP, 1, false, 2>(a, num_sms, s);
+    case LT_SHAPE(2, 2): return launch_op<OP, 2, false, 2>(a, num_sms, s);
+    default: return launch_op<OP, 2, false, 1>(a, num_sms, s);
+    }
+}
+
+int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode, int shape)
 {
     cudaStream_t s = (cudaStream_t)stream;
     if (list_mode) {
         if (op != OP_HESS) return (int)cudaErrorInvalidValue;
-        return launch_op<OP_HESS, 1, true>(args, num_sms, s);
+        return launch_op<OP_HESS, 1, true, 2>(args, num_sms, s);
     }
     switch (op) {
-    case OP_GRAD: return launch_op<OP_GRAD, 2>(args, num_sms, s);
-    case OP_HESS: return launch_op<OP_HESS, 2>(args, num_sms, s);
-    case OP_POT: return launch_op<OP_POT, 2>(args, num_sms, s);
-    case OP_HESS | OP_POT: return launch_op<OP_HESS | OP_POT, 2>(args, num_sms, s);
+    case OP_GRAD: return launch_shape<OP_GRAD>(shape, args, num_sms, s);
+    case OP_HESS: return launch_shape<OP_HESS>(shape, args, num_sms, s);
+    case OP_POT: return launch_shape<OP_POT>(shape, args, num_sms, s);
+    case OP_HESS | OP_POT: return launch_shape<OP_HESS | OP_POT>(shape, args, num_sms, s);
     default: return (int)cudaErrorInvalidValue;
     }
 }
@@ -207,7 +218,7 @@ namespace lt {
 int launch_grid64_list(int op, GridArgs &a, int num_sms, void *stream)
 {
     a.vec_ok = 0;
-    return launch_grid64(op, a, num_sms, stream, true);
+    return launch_grid64(op, a, num_sms, stream, true, LT_SHAPE(1, 2));
 }
 
 /* Maps of an empty catalogue: the epilogue evaluated on zero sums. */

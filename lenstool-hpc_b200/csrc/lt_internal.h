@@ -24,6 +24,7 @@ struct lt_context {
     void *ext = nullptr;       /* state of the batch and serving extensions */
     void *list = nullptr;      /* pixel list of the FP32C recomputation pass (+ count) */
     size_t list_bytes = 0;
+    int shape[2][8] = {};      /* kernel shape per [precision][sums mask], LT_SHAPE() */
 };
 
 struct lt_catalog {
@@ -52,7 +53,7 @@ std::vector<lt_chunk> make_chunks(const int32_t *type, int n, int max_chunk);
 
 lt_status run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g, int precision, int op, int kmap, double D,
                    double mult, double scale, int nout, const int *kinds, double *const *outs, void *stream);
-int launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream);
+int launch_grid64_tiled(int op, GridArgs &a, int num_sms, void *stream, int shape);
 int launch_epilogue_zero(const GridArgs &a, int num_sms, void *stream);
 int launch_grid64_list(int op, GridArgs &a, int num_sms, void *stream);
 /* map kind `kind` of device planes a (xx), b (xy), c (yy) into `out` (in place allowed) */
