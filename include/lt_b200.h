@@ -17,10 +17,10 @@
  *     or host pointers (the library stages through device memory, copies back and
  *     synchronises `stream` before returning, like the reference's host wrappers).
  *   - `stream` is a cudaStream_t passed as void*; NULL means the legacy default stream.
- *   - Precision: LT_FP64 reproduces the reference FP64 CPU path to <= 1e-12 (relative
- *     to max(|value|, RMS of the map)); LT_FP32C runs the bulk halo sum in FP32 with
- *     compensated accumulation and keeps FP64 for cluster-scale halos, near-core pairs and
- *     pixels near critical curves (the error against FP64 is reported by the tests).
+ *   - Precision (lt_precision below): LT_FP64 reproduces the reference FP64 CPU path (the
+ *     Hessian bit for bit); LT_FP32C runs the bulk halo sum in FP32 with compensated
+ *     accumulation and keeps FP64 for cluster-scale halos, near-field pairs and pixels near
+ *     critical curves (its error against FP64 is bounded by the tests).
  */
 #ifndef LT_B200_H
 #define LT_B200_H
@@ -48,7 +48,14 @@ typedef enum {
     LT_ERR_NOT_READY = 10          /* asynchronous result not yet available */
 } lt_status;
 
-typedef enum { LT_FP64 = 0, LT_FP32C = 1 } lt_precision;
+/* LT_FP64: the reference's FP64 arithmetic; the Hessian sums reproduce its rounding
+ *          sequence (bit-identical to the reference CPU path), deflection and potential
+ *          agree to <= 1e-12.
+ * LT_FP32C: FP32 bulk with compensated accumulation and FP64 where FP32 loses digits.
+ * LT_FP64_FAST: FP64 with reciprocals, FMA and shared sub-expressions; as accurate as
+ *          LT_FP64 on average, but its rounding differs, so at the formula's
+ *          ill-conditioned pixels it departs from the reference by up to ~1e-11. */
+typedef enum { LT_FP64 = 0, LT_FP32C = 1, LT_FP64_FAST = 2 } lt_precision;
 
 /* Map kinds computed from the Hessian [[a, b], [d, c]] with D = dlsds (D_LS/D_OS).
  * Reference kernels: ampli src/grid_map_ampli_GPU.cu:329-547, shear

@@ -26,8 +26,8 @@ LIB_PATH = PKG / "liblt_b200.so"
 STATUS = {0: "LT_OK", 1: "LT_ERR_INVALID_ARGUMENT", 2: "LT_ERR_UNKNOWN_PROFILE", 3: "LT_ERR_NONFINITE",
           4: "LT_ERR_CUDA", 5: "LT_ERR_OUT_OF_MEMORY", 6: "LT_ERR_BUDGET", 7: "LT_ERR_QUEUE_FULL",
           8: "LT_ERR_TIMEOUT", 9: "LT_ERR_NO_DEVICE", 10: "LT_ERR_NOT_READY"}
-FP64, FP32C = 0, 1
-PRECISION = {"fp64": FP64, "fp32c": FP32C, FP64: FP64, FP32C: FP32C}
+FP64, FP32C, FP64_FAST = 0, 1, 2
+PRECISION = {"fp64": FP64, "fp32c": FP32C, "fp64fast": FP64_FAST, FP64: FP64, FP32C: FP32C, FP64_FAST: FP64_FAST}
 
 # lt_map_kind
 MAP = {"hess_a": 0, "hess_b": 1, "hess_c": 2, "hess_d": 3,

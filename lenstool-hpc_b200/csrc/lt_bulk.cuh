@@ -102,9 +102,10 @@ __device__ __forceinline__ void eigen2(double A, double B, double C, double &lam
     mu = .5 * (A + C - e);
 }
 
-/* Value of one output plane at one pixel from the pixel's sums. */
-__device__ __forceinline__ double map_value(int kind, double gx, double gy, double hxx, double hyy, double hxy,
-                                            double psi, double D, double mult, double scale)
+/* Value of one output plane at one pixel from the pixel's sums (hyx: the Hessian's d
+ * entry, equal to hxy up to rounding). */
+__device__ __forceinline__ double map_value4(int kind, double gx, double gy, double hxx, double hyy, double hxy,
+                                             double hyx, double psi, double D, double mult, double scale)
 {
     double a = hxx, b = hxy, c = hyy;
     double lam, mu;
@@ -112,7 +113,7 @@ __device__ __forceinline__ double map_value(int kind, double gx, double gy, doub
     case LT_MAP_HESS_A: return a;
     case LT_MAP_HESS_B: return b;
     case LT_MAP_HESS_C: return c;
-    case LT_MAP_HESS_D: return b;
+    case LT_MAP_HESS_D: return hyx;
     case LT_MAP_AMPLI1: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return 1. / (lam * mu);
     case LT_MAP_AMPLI2: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return 1. / fabs(lam * mu);
     case LT_MAP_AMPLI3: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return -2.5 * log10(fabs(lam * mu));
@@ -152,6 +153,12 @@ __device__ __forceinline__ double map_value(int kind, double gx, double gy, doub
     case KIND_POT: return psi * scale;
     default: return 0.;
     }
+}
+
+__device__ __forceinline__ double map_value(int kind, double gx, double gy, double hxx, double hyy, double hxy,
+                                            double psi, double D, double mult, double scale)
+{
+    return map_value4(kind, gx, gy, hxx, hyy, hxy, hxy, psi, D, mult, scale);
 }
 
 } // namespace lt

@@ -190,19 +190,22 @@ static lt_status validate(lt_context *ctx, const lt_halo_soa *s)
     return LT_OK;
 }
 
-std::vector<lt_chunk> lt::make_chunks(const int32_t *type, int n, int max_chunk)
+/* Runs of equal type (and, with `dlsds`, equal D_LS/D_OS: the Kmap's runs,
+ * src/gradient2_GPU.cu:484-512) split into chunks of at most max_chunk halos; the last
+ * chunk of each run carries CHUNK_RUN_END. */
+std::vector<lt_chunk> lt::make_chunks(const int32_t *type, int n, int max_chunk, const double *dlsds)
 {
     std::vector<lt_chunk> ch;
     int s = 0;
     while (s < n) {
         int e = s + 1;
-        while (e < n && type[e] == type[s]) e++;
+        while (e < n && type[e] == type[s] && (!dlsds || dlsds[e] == dlsds[s])) e++;
         for (int c = s; c < e; c += max_chunk) {
             lt_chunk k;
             k.start = c;
             k.count = (e - c) < max_chunk ? (e - c) : max_chunk;
             k.type = type[s];
-            k.pad = 0;
+            k.pad = (c + k.count == e) ? CHUNK_RUN_END : 0;
             ch.push_back(k);
         }
         s = e;
@@ -254,13 +257,19 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
     if (!ctx) return LT_ERR_OUT_OF_MEMORY;
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
-    /* default kernel shapes (pixels per thread, CTAs per SM); lt_autotune refines them */
-    for (int p = 0; p < 2; p++)
+    /* default kernel shapes (pixels per thread, CTAs per SM), from a sweep on B200 at
+     * 1024^2 x 1000 halos; lt_autotune refines them for a given catalogue */
+    for (int p = 0; p < 3; p++)
         for (int o = 0; o < 8; o++) ctx->shape[p][o] = LT_SHAPE(2, 1);
-    ctx->shape[LT_FP64][OP_POT] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP64][OP_HESS | OP_POT] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP64][OP_HESS] = LT_SHAPE(1, 2);
+    ctx->shape[LT_FP64][OP_POT] = LT_SHAPE(1, 1);
+    ctx->shape[LT_FP64][OP_HESS | OP_POT] = LT_SHAPE(1, 2);
+    ctx->shape[LT_FP64][OP_GRAD] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP64_FAST][OP_POT] = LT_SHAPE(1, 1);
+    ctx->shape[LT_FP64_FAST][OP_HESS | OP_POT] = LT_SHAPE(1, 1);
+    ctx->shape[LT_FP64_FAST][OP_GRAD] = LT_SHAPE(2, 2);
     ctx->shape[LT_FP32C][OP_HESS] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE(2, 2);
     ctx->shape[LT_FP32C][OP_HESS | OP_POT] = LT_SHAPE(2, 2);
     cudaSetDevice(device);
     size_t free_b = 0, total_b = 0;
@@ -310,14 +319,21 @@ lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *s, lt_catalog **
     cat->host_types.assign(s->type, s->type + s->nhalos);
     for (int i = 0; i < s->nhalos; i++) pack_one(s, i, cat->host_recs[i]);
     std::vector<lt_chunk> ch = make_chunks(s->type, s->nhalos, LT_CHUNK);
+    std::vector<double> w(s->nhalos);
+    for (int i = 0; i < s->nhalos; i++) w[i] = cat->host_recs[i].w;
+    std::vector<lt_chunk> chk = make_chunks(s->type, s->nhalos, LT_CHUNK, w.data());
     cat->nchunks = (int32_t)ch.size();
-    size_t rb = sizeof(lt_rec64) * (size_t)s->nhalos, cb = sizeof(lt_chunk) * ch.size();
+    cat->nchunks_k = (int32_t)chk.size();
+    size_t rb = sizeof(lt_rec64) * (size_t)s->nhalos, cb = sizeof(lt_chunk) * (ch.size() + chk.size());
     cat->bytes = rb + cb;
     st = dev_alloc(ctx, (void **)&cat->recs, rb);
     if (st == LT_OK) st = dev_alloc(ctx, (void **)&cat->chunks, cb);
+    cat->chunks_k = cat->chunks + ch.size();
     if (st == LT_OK && rb) {
         cudaError_t e = cudaMemcpy(cat->recs, cat->host_recs.data(), rb, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && cb) e = cudaMemcpy(cat->chunks, ch.data(), cb, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(cat->chunks, ch.data(), sizeof(lt_chunk) * ch.size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(cat->chunks_k, chk.data(), sizeof(lt_chunk) * chk.size(), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) st = cuda_fail(ctx, e, "catalogue upload");
     }
     if (st == LT_OK) st = prepare_catalog_extensions(ctx, cat);
@@ -335,7 +351,7 @@ lt_status lt_catalog_release(lt_context *ctx, lt_catalog *cat)
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     dev_free(ctx, cat->recs, sizeof(lt_rec64) * (size_t)cat->nhalos);
-    dev_free(ctx, cat->chunks, sizeof(lt_chunk) * (size_t)cat->nchunks);
+    dev_free(ctx, cat->chunks, sizeof(lt_chunk) * (size_t)(cat->nchunks + cat->nchunks_k));
     dev_free(ctx, cat->aux, cat->aux_bytes);
     delete cat;
     return LT_OK;
@@ -379,7 +395,7 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
         if (ctx) set_error(ctx, "invalid grid-call arguments");
         return LT_ERR_INVALID_ARGUMENT;
     }
-    if (precision != LT_FP64 && precision != LT_FP32C) {
+    if (precision != LT_FP64 && precision != LT_FP32C && precision != LT_FP64_FAST) {
         set_error(ctx, "unknown precision %d", precision);
         return LT_ERR_INVALID_ARGUMENT;
     }
@@ -404,8 +420,8 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
     GridArgs a;
     memset(&a, 0, sizeof(a));
     a.recs = cat->recs;
-    a.chunks = cat->chunks;
-    a.nchunks = cat->nchunks;
+    a.chunks = kmap ? cat->chunks_k : cat->chunks;
+    a.nchunks = kmap ? cat->nchunks_k : cat->nchunks;
     a.kmap = kmap;
     a.xmin = g->xmin;
     a.ymin = g->ymin;
@@ -437,7 +453,11 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
             count_launch(1);
         }
     } else if (precision == LT_FP64) {
-        err = launch_grid64_tiled(op, a, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
+        /* the Hessian with the reference's rounding sequence */
+        const int xop = (op & OP_HESS) ? ((op & ~OP_HESS) | OP_HEX) : op;
+        err = launch_grid64_tiled(xop, a, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
+    } else if (precision == LT_FP64_FAST) {
+        err = launch_grid64_tiled(op, a, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][op & 7]);
     } else {
         err = launch_fp32c(ctx, cat, op, a, s);
     }
@@ -537,8 +557,9 @@ lt_status lt_lens_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *gr
 
 static bool sums_ok(int precision, int sums)
 {
-    if (precision != LT_FP64 && precision != LT_FP32C) return false;
-    if (precision == LT_FP64) return sums == OP_GRAD || sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
+    if (precision != LT_FP64 && precision != LT_FP32C && precision != LT_FP64_FAST) return false;
+    if (precision != LT_FP32C)
+        return sums == OP_GRAD || sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
     return sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
 }
 

@@ -15,8 +15,12 @@ enum {
     KIND_POT = 102     /* potential * scale */
 };
 
-/* which sums a kernel evaluates */
-enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4 };
+/* which sums a kernel evaluates; OP_HEX is the Hessian with the reference's rounding
+ * sequence (LT_FP64), OP_HESS the reformulated one (LT_FP64_FAST and the FP32C path) */
+enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4, OP_HEX = 8 };
+
+/* chunk.pad bits: FP32 records (FP32C list), last chunk of a run */
+enum { CHUNK_FP32 = 1, CHUNK_RUN_END = 2 };
 
 struct GridArgs {
     const lt_rec64 *recs;

@@ -44,7 +44,7 @@ static const double kTau = 0.1;        /* FP64 where b0 / (2 r) > kTau          
 static const double kSingFrac = 0.3;
 static const double kSingEps = 1.5;
 static const double kCoreFrac = 3.0;   /* FP64 within 3 rcore of the centre           */
-static const double kMuFlag = 4.0;     /* recompute pixels with |mu| above this       */
+static const double kMuFlag = 2.5;     /* recompute pixels with |mu| above this (error ~ mu^2) */
 
 static bool needs_fp64_always(const lt_rec64 &r, int type)
 {
@@ -142,13 +142,13 @@ lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
         c.start = idx64_always[k];
         c.count = (int32_t)(e - k);
         c.type = t64[k];
-        c.pad = 0;
+        c.pad = 0; /* FP64 records; the fast Hessian needs no run boundaries */
         host_chunks.push_back(c);
         k = e;
     }
     std::vector<lt_chunk> c32 = make_chunks(t32.data(), (int)t32.size(), LT_CHUNK);
     for (lt_chunk c : c32) {
-        c.pad = 1;
+        c.pad = CHUNK_FP32;
         host_chunks.push_back(c);
     }
     Fp32cCatalog h;
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args
         uint64_t *bar = &bars[s & 1];
         const void *src;
         uint32_t bytes;
-        if (c.pad) {
+        if (c.pad & CHUNK_FP32) {
             src = A.recs32 + c.start;
             bytes = (uint32_t)c.count * (uint32_t)sizeof(lt_rec32);
         } else {
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args
 
         const lt_chunk c = A.chunks[ci];
         const unsigned char *buf = b ? buf1 : buf0;
-        if (c.pad) {
+        if (c.pad & CHUNK_FP32) {
             const lt_rec32 *recs = reinterpret_cast<const lt_rec32 *>(buf);
             switch (c.type) {
             case 81: eval32_chunk<OP, P, 81>(recs, a.recs, c.count, px, py, a.kmap, acc); break;

@@ -25,6 +25,7 @@ constexpr int kThreads = 256;
 template <int OP, int P>
 struct Acc64 {
     double gx[P], gy[P], hxx[P], hyy[P], hxy[P], psi[P];
+    ex::Mat run[P], tot[P]; /* OP_HEX: the reference's per-run and total sums */
 };
 
 template <int OP, int P, int TYPE>
@@ -45,8 +46,34 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
                 acc.hyy[k] = hh.yy;
                 acc.hxy[k] = hh.xy;
             }
+            if (OP & OP_HEX) ex::hess_pair<TYPE>(r, px[k], py, acc.run[k]);
             if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
         }
+    }
+}
+
+/* End of a run of the reference's dispatch (src/gradient2.cpp:240-251): the run's sum
+ * joins the total, weighted by the run's dlsds for the Kmap
+ * (src/gradient2_GPU.cu:503-507). */
+template <int OP, int P>
+__device__ __forceinline__ void close_run64(Acc64<OP, P> &acc, int kmap, double w)
+{
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        ex::Mat &t = acc.tot[k];
+        const ex::Mat &r = acc.run[k];
+        if (kmap) {
+            t.a = ex::A(t.a, ex::M(r.a, w));
+            t.b = ex::A(t.b, ex::M(r.b, w));
+            t.c = ex::A(t.c, ex::M(r.c, w));
+            t.d = ex::A(t.d, ex::M(r.d, w));
+        } else {
+            t.a = ex::A(t.a, r.a);
+            t.b = ex::A(t.b, r.b);
+            t.c = ex::A(t.c, r.c);
+            t.d = ex::A(t.d, r.d);
+        }
+        acc.run[k].a = acc.run[k].b = acc.run[k].c = acc.run[k].d = 0.;
     }
 }
 
@@ -119,6 +146,8 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
                 const int cx = (ix + k) < a.nx ? ix + k : a.nx - 1;
                 px[k] = pixel_x(a, cx);
                 acc.gx[k] = acc.gy[k] = acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
+                acc.run[k].a = acc.run[k].b = acc.run[k].c = acc.run[k].d = 0.;
+                acc.tot[k].a = acc.tot[k].b = acc.tot[k].c = acc.tot[k].d = 0.;
             }
         }
         if (tid == 0 && s + 1 < steps) issue(s + 1);
@@ -140,16 +169,25 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
         case 5: eval_chunk64<OP, P, 5>(recs, c.count, px, py, a.kmap, acc); break;
         default: break;
         }
+        if ((OP & OP_HEX) && (c.pad & CHUNK_RUN_END)) close_run64<OP, P>(acc, a.kmap, recs[c.count - 1].w);
 
         if (ci == a.nchunks - 1 && iy < a.ny) {
             const long row = (long)iy * a.nx;
             const bool full = a.vec_ok && (ix + P <= a.nx);
+            if (OP & OP_HEX) {
+#pragma unroll
+                for (int k = 0; k < P; k++) {
+                    acc.hxx[k] = acc.tot[k].a;
+                    acc.hxy[k] = acc.tot[k].b;
+                    acc.hyy[k] = acc.tot[k].c;
+                }
+            }
             for (int o = 0; o < a.nout; o++) {
                 double v[P];
 #pragma unroll
                 for (int k = 0; k < P; k++)
-                    v[k] = map_value(a.kinds[o], acc.gx[k], acc.gy[k], acc.hxx[k], acc.hyy[k], acc.hxy[k], acc.psi[k],
-                                     a.D, a.mult, a.scale);
+                    v[k] = map_value4(a.kinds[o], acc.gx[k], acc.gy[k], acc.hxx[k], acc.hyy[k], acc.hxy[k],
+                                      (OP & OP_HEX) ? acc.tot[k].d : acc.hxy[k], acc.psi[k], a.D, a.mult, a.scale);
                 double *dst = a.out[o] + row + ix;
                 if (P == 2 && full) {
                     *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1 % P]);
@@ -207,6 +245,8 @@ int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool 
     case OP_HESS: return launch_shape<OP_HESS>(shape, args, num_sms, s);
     case OP_POT: return launch_shape<OP_POT>(shape, args, num_sms, s);
     case OP_HESS | OP_POT: return launch_shape<OP_HESS | OP_POT>(shape, args, num_sms, s);
+    case OP_HEX: return launch_shape<OP_HEX>(shape, args, num_sms, s);
+    case OP_HEX | OP_POT: return launch_shape<OP_HEX | OP_POT>(shape, args, num_sms, s);
     default: return (int)cudaErrorInvalidValue;
     }
 }

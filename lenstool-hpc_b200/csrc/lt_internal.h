@@ -24,14 +24,15 @@ struct lt_context {
     void *ext = nullptr;       /* state of the batch and serving extensions */
     void *list = nullptr;      /* pixel list of the FP32C recomputation pass (+ count) */
     size_t list_bytes = 0;
-    int shape[2][8] = {};      /* kernel shape per [precision][sums mask], LT_SHAPE() */
+    int shape[3][8] = {};      /* kernel shape per [precision][sums mask], LT_SHAPE() */
 };
 
 struct lt_catalog {
     lt_rec64 *recs = nullptr;            /* FP64 records, device */
-    lt_chunk *chunks = nullptr;          /* FP64 chunk list, device */
+    lt_chunk *chunks = nullptr;          /* FP64 chunk list (runs of one type), device */
+    lt_chunk *chunks_k = nullptr;        /* Kmap chunk list (runs of one type and dlsds) */
     int32_t nhalos = 0;
-    int32_t nchunks = 0;
+    int32_t nchunks = 0, nchunks_k = 0;
     size_t bytes = 0;
     std::vector<lt_rec64> host_recs;     /* packed records, host copy */
     std::vector<int32_t> host_types;     /* profile type per halo */
@@ -49,7 +50,7 @@ lt_status dev_alloc(lt_context *ctx, void **p, size_t bytes);
 void dev_free(lt_context *ctx, void *p, size_t bytes);
 lt_status scratch_planes(lt_context *ctx, int n, size_t plane_bytes, double **planes);
 bool is_device_pointer(const void *p);
-std::vector<lt_chunk> make_chunks(const int32_t *type, int n, int max_chunk);
+std::vector<lt_chunk> make_chunks(const int32_t *type, int n, int max_chunk, const double *dlsds = nullptr);
 
 lt_status run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g, int precision, int op, int kmap, double D,
                    double mult, double scale, int nout, const int *kinds, double *const *outs, void *stream);

@@ -219,3 +219,98 @@ __device__ __forceinline__ void pot_pair(const lt_rec64 &h, double px, double py
 }
 
 } // namespace lt
+
+/* ------------------------------------------------ reference-exact Hessian ---- */
+/* The reference's Hessian arithmetic with its rounding sequence: every operation is a
+ * separately rounded IEEE operation (no contraction into FMA, true division and square
+ * root), in C's left-to-right evaluation order.  The results are bit-identical to the
+ * reference FP64 CPU path (src/gradient2.cpp:54-205), whose formula is ill-conditioned
+ * near each halo's removable singular points and near small-ellipticity cores: any other
+ * rounding sequence differs there by up to ~1e-12 of the map scale. */
+namespace lt {
+namespace ex {
+__device__ __forceinline__ double M(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double A(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double S(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double V(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double R(double a) { return __dsqrt_rn(a); }
+
+struct Mat {
+    double a, b, c, d;
+};
+
+/* mdci05_hpc, src/gradient2.cpp:54-83 */
+__device__ __forceinline__ Mat mdci05(double x, double y, double eps, double rc, double b0)
+{
+    const double sqe = R(eps);
+    const double cx1 = V(S(1., eps), A(1., eps));
+    const double cx1inv = V(1., cx1);
+    const double cxro = M(A(1., eps), A(1., eps));
+    const double cyro = M(S(1., eps), S(1., eps));
+    const double ci = V(M(0.5, S(1., M(eps, eps))), sqe);
+    const double wrem = R(A(A(M(rc, rc), V(M(x, x), cxro)), V(M(y, y), cyro)));
+    const double sq2 = M(2., sqe);
+    double den1 = S(M(sq2, wrem), M(y, cx1inv));
+    den1 = A(M(M(M(cx1, cx1), x), x), M(den1, den1));
+    const double num2 = S(M(M(2., rc), sqe), y);
+    const double den2 = A(M(x, x), M(num2, num2));
+    double t = A(S(V(V(M(M(sq2, x), x), cxro), wrem), M(sq2, wrem)), M(y, cx1inv));
+    const double didxre = M(ci, A(V(M(cx1, t), den1), V(num2, den2)));
+    t = S(V(V(M(M(M(sq2, x), y), cx1), cyro), wrem), x);
+    const double didyre = M(ci, A(V(t, den1), V(x, den2)));
+    t = S(M(M(sq2, wrem), cx1inv), M(M(y, cx1inv), cx1inv));
+    t = S(t, V(M(M(4., eps), y), cyro));
+    t = A(t, M(V(V(M(M(sq2, y), y), cyro), wrem), cx1inv));
+    const double didyim = M(ci, S(V(t, den1), V(num2, den2)));
+    Mat r;
+    r.a = M(b0, didxre);
+    r.b = r.d = M(b0, didyre);
+    r.c = M(b0, didyim);
+    return r;
+}
+
+/* two-step rotation back to the sky frame, src/gradient2.cpp:146-156 */
+__device__ __forceinline__ void rotate_acc(const Mat &h, double cs, double sn, Mat &acc)
+{
+    const double ma = A(M(h.a, cs), M(h.b, -sn));
+    const double mb = A(M(h.a, sn), M(h.b, cs));
+    const double mc = A(M(h.d, sn), M(h.c, cs));
+    const double md = A(M(h.d, cs), M(h.c, -sn));
+    acc.a = A(acc.a, S(M(cs, ma), M(sn, md)));
+    acc.b = A(acc.b, S(M(cs, mb), M(sn, mc)));
+    acc.c = A(acc.c, A(M(sn, mb), M(cs, mc)));
+    acc.d = A(acc.d, A(M(sn, ma), M(cs, md)));
+}
+
+/* One halo's Hessian added to the run accumulator `acc`: dPIE src/gradient2.cpp:92-205;
+ * PIEMD (one mdci05 term) and SIS restated with the same rounding discipline. */
+template <int TYPE>
+__device__ __forceinline__ void hess_pair(const lt_rec64 &h, double px, double py, Mat &acc)
+{
+    const double tx = S(px, h.x0), ty = S(py, h.y0);
+    const double u = A(M(tx, h.cs), M(ty, h.sn));
+    const double v = S(M(ty, h.cs), M(tx, h.sn));
+    Mat m;
+    if (TYPE == 81) {
+        const double t05 = V(h.rcut, S(h.rcut, h.rc));
+        Mat core = mdci05(u, v, h.eps, h.rc, h.b0);
+        const Mat cut = mdci05(u, v, h.eps, h.rcut, h.b0);
+        m.a = M(t05, S(core.a, cut.a));
+        m.b = M(t05, S(core.b, cut.b));
+        m.c = M(t05, S(core.c, cut.c));
+        m.d = M(t05, S(core.d, cut.d));
+    } else if (TYPE == 8) {
+        m = mdci05(u, v, h.eps, h.rc, h.b0);
+    } else {
+        const double e = h.eps;
+        const double q = A(M(M(u, u), S(1., e)), M(M(v, v), A(1., e)));
+        const double r = R(q);
+        const double k = V(M(M(h.b0, S(1., e)), A(1., e)), M(q, r));
+        m.a = M(M(k, v), v);
+        m.c = M(M(k, u), u);
+        m.b = m.d = M(M(-k, u), v);
+    }
+    rotate_acc(m, h.cs, h.sn, acc);
+}
+} // namespace ex
+} // namespace lt

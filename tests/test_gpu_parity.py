@@ -49,7 +49,8 @@ def test_par_dpie_hessian_potential_kmap(ctx):
     cat, g = catalog_from_npz(z), grid_from_npz(z)
     m = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "hess_d", "ampli5"])
     for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
-        assert max_rel_err(m[name], z["hess"][k]) <= TOL
+        # bit-identical to the reference's gradient2_grid_CPU
+        assert np.array_equal(m[name], z["hess"][k]), name
     assert max_rel_err(m["ampli5"], z["amplif5"]) <= TOL
     psi = ctx.potential_grid(cat, g)
     assert max_rel_err(psi, z["pot"]) <= TOL
@@ -57,7 +58,8 @@ def test_par_dpie_hessian_potential_kmap(ctx):
     kcat.dlsds = np.array(z["kmap_dlsds"])
     mk = ctx.hessian_maps(kcat, g, ["hess_a", "hess_b", "hess_c", "hess_d"], kmap=True)
     for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
-        assert max_rel_err(mk[name], z["kmap"][k]) <= TOL
+        # bit-identical to the reference's Kmap kernel (run on the host)
+        assert np.array_equal(mk[name], z["kmap"][k]), name
 
 
 def _cat(cluster_type=81, n_gal=198, seed=20261203):
@@ -76,7 +78,11 @@ def test_grid_vs_oracle(ctx, oracle_lib, cluster_type, shape):
     h = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "hess_d"])
     oh = oracle_lib.hess_grid(cat, g)
     for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
-        assert max_rel_err(h[name], oh[k]) <= TOL, name
+        # LT_FP64 reproduces the reference's rounding sequence: bit-identical planes
+        assert np.array_equal(h[name], oh[k]), (name, max_rel_err(h[name], oh[k]))
+    hf = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c"], precision="fp64fast")
+    for k, name in enumerate(["hess_a", "hess_b", "hess_c"]):
+        assert max_rel_err(hf[name], oh[k]) <= TOL, name
     psi = ctx.potential_grid(cat, g)
     assert max_rel_err(psi, oracle_lib.pot_grid(cat, g)) <= TOL
 
@@ -130,9 +136,9 @@ def test_kmap_multi_plane_vs_oracle(ctx, oracle_lib):
     g = catalog.Grid.square(80., 48)
     m = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "mass"], kmap=True, mult=2.)
     oh = oracle_lib.hess_grid(cat, g, kmap=True)
-    assert max_rel_err(m["hess_a"], oh[0]) <= TOL
-    assert max_rel_err(m["hess_b"], oh[1]) <= TOL
-    assert max_rel_err(m["hess_c"], oh[2]) <= TOL
+    assert np.array_equal(m["hess_a"], oh[0])
+    assert np.array_equal(m["hess_b"], oh[1])
+    assert np.array_equal(m["hess_c"], oh[2])
     assert max_rel_err(m["mass"], (oh[0] + oh[2]) * 0.5 * 2.) <= 1e-12
 
 
@@ -178,15 +184,7 @@ def test_errors_are_statuses(ctx):
     small.close()
 
 
-def test_c1_scale_subsample_fp64(ctx, oracle_lib):
-    """1000 halos on the 4096^2 grid: the FP64 Hessian maps on a pixel subsample
-    (65536 seeded pixels plus every pixel within 3 rcore of a halo centre)."""
-    import torch
-    cat, g = catalog.workload("maps_1000h_4096")
-    D = 0.6
-    outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in ("kappa", "gamma1", "gamma2")}
-    ctx.hessian_maps(ctx.upload(cat), g, list(outs), dlsds=D, out=list(outs.values()))
-    ctx.synchronize()
+def _c1_subsample(cat, g):
     rng = np.random.default_rng(20261204)
     idx = rng.choice(g.npix, 65536, replace=False)
     near = []
@@ -196,14 +194,45 @@ def test_c1_scale_subsample_fp64(ctx, oracle_lib):
         for jj in range(max(0, j - r), min(g.ny, j + r + 1)):
             for ii in range(max(0, i - r), min(g.nx, i + r + 1)):
                 near.append(jj * g.nx + ii)
-    idx = np.unique(np.concatenate([idx, np.array(near, np.int64)]))
+    return np.unique(np.concatenate([idx, np.array(near, np.int64)]))
+
+
+def test_c1_scale_subsample_fp64_exact(ctx, oracle_lib):
+    """1000 halos on the 4096^2 grid, LT_FP64: kappa, gamma1, gamma2 equal the reference's
+    FP64 arithmetic bit for bit on a pixel subsample (65536 seeded pixels plus every
+    pixel within 3 rcore of a halo centre)."""
+    import torch
+    cat, g = catalog.workload("maps_1000h_4096")
+    D = 0.6
+    outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in ("kappa", "gamma1", "gamma2")}
+    ctx.hessian_maps(ctx.upload(cat), g, list(outs), dlsds=D, out=list(outs.values()))
+    ctx.synchronize()
+    idx = _c1_subsample(cat, g)
+    px, py = g.coords(idx)
+    a, b, c, d = oracle_lib.hess_points(cat, px, py)
+    for k, ref in (("kappa", (a + c) * D / 2), ("gamma1", (a - c) * D / 2), ("gamma2", b * D)):
+        got = outs[k].cpu().numpy().ravel()[idx]
+        assert np.array_equal(got, ref), (k, int((got != ref).sum()))
+
+
+def test_c1_scale_subsample_fp64_fast(ctx, oracle_lib):
+    """LT_FP64_FAST on the same subsample: within 1e-12 except where the reference formula
+    is ill-conditioned (bounded by its measured conditioning)."""
+    import torch
+    cat, g = catalog.workload("maps_1000h_4096")
+    D = 0.6
+    outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in ("kappa", "gamma1", "gamma2")}
+    ctx.hessian_maps(ctx.upload(cat), g, list(outs), precision="fp64fast", dlsds=D, out=list(outs.values()))
+    ctx.synchronize()
+    idx = _c1_subsample(cat, g)
     px, py = g.coords(idx)
     a, b, c, d = oracle_lib.hess_points(cat, px, py)
     # The reference formula is ill-conditioned within ~1e-3" of each halo's removable
     # singular points (0, 2 r sqrt(eps)) of the halo frame: there a 1-ulp change of the
     # pixel coordinate moves the reference's own result by up to ~1e-8, and its FP64
     # rounding error (measured against the extended-precision build of the oracle)
-    # grows alike.  Each pixel is held to 1e-12 plus 16x the larger of the two.
+    # grows alike; LT_FP64_FAST rounds differently (as accurately on average), so near
+    # those points each pixel is held to 1e-11 plus 64x the larger of the two.
     import oracle
     ext = oracle.Oracle(oracle.ORACLE_LD_SO).hess_points(cat, px, py)
     pert = [oracle_lib.hess_points(cat, np.nextafter(px, s * np.inf), py) for s in (1, -1)]
@@ -218,7 +247,7 @@ def test_c1_scale_subsample_fp64(ctx, oracle_lib):
         den = np.maximum(np.abs(ref), rms)
         sens = np.max([np.abs(f(p) - ref) for p in pert], axis=0) / den
         err = np.abs(got - ref) / den
-        bad = np.flatnonzero(err > TOL + 16 * sens)
+        bad = np.flatnonzero(err > 10 * TOL + 64 * sens)
         assert bad.size == 0, (k, [(float(err[i]), float(sens[i]), float(px[i]), float(py[i])) for i in bad[:5]])
         # away from those points the plain bound holds
         assert np.max(err[sens < 1e-14]) <= TOL, k
