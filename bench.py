@@ -147,12 +147,193 @@ def reference_cpu(steps, warmup, rows=None):
                "seconds_per_sample": float(np.mean(times))}
 
 
+def _percentile(xs, q):
+    return float(np.percentile(np.asarray(xs, np.float64), q)) if len(xs) else None
+
+
+def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sample=16, e2e=True):
+    """Posterior-batch workload: n_sets Gaussian 5% perturbations (seeded) of the 200-halo
+    catalogue (2 cluster + 198 galaxy halos), each on a grid drawn from {512^2, 1024^2,
+    2048^2} over the 200"x200" field; outputs mu and kappa per set; all sets in one
+    graph-captured persistent launch (lt_batch).  Compared with one map call per set in
+    the reference's calling pattern (upload, compute, copy back, release)."""
+    import torch
+    lt = _package()
+    from lenstool_hpc_b200 import catalog
+    rng = np.random.Generator(np.random.PCG64(20261203 + 2))
+    base = catalog.cluster_galaxy_catalog(2, 198, 20261203)
+    sizes = rng.choice([512, 1024, 2048], n_sets)
+    sets = [catalog.perturb_catalog(base, rng) for _ in range(n_sets)]
+    grids = {n: catalog.Grid.square(100., int(n)) for n in (512, 1024, 2048)}
+    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
+    D = dls / dos
+    kinds = ("mu", "kappa")
+    cats = [ctx.upload(c) for c in sets]
+    outs = [{k: torch.empty((int(n), int(n)), dtype=torch.float64, device="cuda") for k in kinds} for n in sizes]
+    reqs = [lt.Request(c, grids[int(n)], o, dlsds=D) for c, n, o in zip(cats, sizes, outs)]
+    batch = ctx.batch(reqs, precision=precision)
+    evals = float(sum(int(n) * int(n) for n in sizes)) * base.n
+    stream = torch.cuda.Stream()
+    for _ in range(warmup):
+        batch.launch(stream)
+    ctx.synchronize(stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = lt.launch_count()
+    e0.record(stream)
+    for _ in range(steps):
+        batch.launch(stream)
+    e1.record(stream)
+    ctx.synchronize(stream)
+    launches = lt.launch_count() - n0
+    dt = e0.elapsed_time(e1) / 1e3 / steps
+    res = {"workload": f"posterior_batch: {n_sets} sets x {base.n} halos, grids U{{512,1024,2048}}^2, mu+kappa",
+           "precision": precision, "maps_per_s": 2 * n_sets / dt, "sets_per_s": n_sets / dt, "evals_per_s": evals / dt,
+           "ms_per_step": dt * 1e3, "gpu_launches_per_step": launches / steps,
+           "evals_per_step": evals, "l2": f"outputs {2 * 8 * evals / base.n / 1e9:.1f} GB per step > L2"}
+    # one map call per set (upload, compute into pageable host arrays, release): a sample
+    # of the sets, scaled to all sets by their halo x pixel evaluations
+    plain = {}
+    idx = list(range(plain_sample))
+    for prec in ("fp64", precision):
+        host = {i: {k: np.empty((int(sizes[i]), int(sizes[i]))) for k in kinds} for i in idx}
+        c = ctx.upload(sets[0])
+        ctx.hessian_maps(c, grids[int(sizes[0])], list(kinds), precision=prec, dlsds=D, out=list(host[0].values()))
+        c.release()
+        t0 = time.perf_counter()
+        for i in idx:
+            c = ctx.upload(sets[i])
+            ctx.hessian_maps(c, grids[int(sizes[i])], list(kinds), precision=prec, dlsds=D,
+                             out=list(host[i].values()))
+            c.release()
+        t = time.perf_counter() - t0
+        sample_evals = float(sum(int(sizes[i]) ** 2 for i in idx)) * base.n
+        t_all = t * evals / sample_evals
+        plain[prec] = {"maps_per_s": 2 * n_sets / t_all, "sample_sets": len(idx), "sample_s": t}
+    res["one_map_per_call"] = plain
+    res["speedup_vs_one_map_per_call_fp64"] = res["maps_per_s"] / plain["fp64"]["maps_per_s"]
+    res["speedup_vs_one_map_per_call_same_precision"] = res["maps_per_s"] / plain[precision]["maps_per_s"]
+    try:
+        import psutil
+        host_free = psutil.virtual_memory().available
+    except Exception:
+        host_free = 0
+    if e2e and host_free < 3 * 2 * 8 * evals / base.n:
+        res["e2e"] = {"skipped": f"host memory available {host_free / 1e9:.0f} GB < 3x the maps"}
+        e2e = False
+    if e2e:
+        # end to end through the public API: the sets' catalogues uploaded from host arrays,
+        # the batch built (graph captured), launched, and every map copied to host memory
+        host = [{k: torch.empty((int(n), int(n)), dtype=torch.float64).numpy() for k in kinds} for n in sizes]
+        t0 = time.perf_counter()
+        cats2 = [ctx.upload(c) for c in sets]
+        b2 = ctx.batch([lt.Request(c, grids[int(n)], o, dlsds=D) for c, n, o in zip(cats2, sizes, outs)],
+                       precision=precision)
+        b2.launch(stream)
+        ctx.synchronize(stream)
+        for o, h in zip(outs, host):
+            for k in kinds:
+                torch.from_numpy(h[k]).copy_(o[k])
+        b2.destroy()
+        for c in cats2:
+            c.release()
+        te = time.perf_counter() - t0
+        res["e2e"] = {"maps_per_s": 2 * n_sets / te, "h2d_bytes_per_step": n_sets * base.n * (192 + 160),
+                      "d2h_bytes_per_step": int(2 * 8 * evals / base.n),
+                      "note": "upload of every set's catalogue + batch build + launch + maps to pageable host"}
+        res["e2e"]["speedup_vs_one_map_per_call_fp64"] = res["e2e"]["maps_per_s"] / plain["fp64"]["maps_per_s"]
+    batch.destroy()
+    for c in cats:
+        c.release()
+    return res
+
+
+def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=8, seed=20261203 + 4):
+    """Serving workload: Poisson arrivals at `rate` req/s of requests drawn uniformly from
+    {deflection map, kappa/gamma1/gamma2/mu maps}, grids U{512^2, 1024^2, 2048^2, 4096^2},
+    catalogues with log-uniform(50, 5000) halos (1% cluster-scale) resident in HBM.  The
+    serving loop's p50/p99 latency (submission to results in HBM) and maps/s, against the
+    same requests as one plain FP64 call each."""
+    import torch
+    lt = _package()
+    from lenstool_hpc_b200 import catalog
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pool = []
+    for i in range(12):
+        n = int(round(np.exp(rng.uniform(np.log(50.), np.log(5000.)))))
+        nc = max(1, int(round(0.01 * n)))
+        pool.append(catalog.cluster_galaxy_catalog(nc, n - nc, seed + 100 + i))
+    dcats = [ctx.upload(c) for c in pool]
+    kinds_of = (("deflection_x", "deflection_y"), ("kappa", "gamma1", "gamma2", "mu"))
+    reqs = []
+    for i in range(n_requests):
+        k = int(rng.integers(2))
+        n = int(rng.choice([512, 1024, 2048, 4096]))
+        c = int(rng.integers(len(pool)))
+        reqs.append((k, n, c))
+    gaps = rng.exponential(1.0 / rate, n_requests)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
+    D = dls / dos
+    outs = [{kk: torch.empty((n, n), dtype=torch.float64, device="cuda") for kk in kinds_of[k]} for k, n, c in reqs]
+    evals = float(sum(n * n * pool[c].n for k, n, c in reqs))
+    nmaps = sum(len(kinds_of[k]) for k, n, c in reqs)
+
+    def run(arr):
+        with ctx.server(precision=precision, slots=64, window=8) as srv:
+            # warm-up request (the loop kernel's first launch)
+            w = {"kappa": torch.empty((64, 64), dtype=torch.float64, device="cuda")}
+            srv.wait(srv.submit(lt.Request(dcats[0], catalog.Grid.square(100., 64), w, dlsds=D)))
+            tickets = []
+            t0 = time.perf_counter()
+            for (k, n, c), o, ta in zip(reqs, outs, arr):
+                now = time.perf_counter() - t0
+                if ta > now:
+                    time.sleep(ta - now)
+                tickets.append(srv.submit(lt.Request(dcats[c], catalog.Grid.square(100., n), o, dlsds=D, scale=D)))
+            for t in tickets:
+                srv.wait(t, 3600.)
+            t_end = time.perf_counter() - t0
+            lat = [srv.times(t)[2] for t in tickets]
+            st = srv.stats()
+        return {"p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99), "maps_per_s": nmaps / t_end,
+                "requests_per_s": len(reqs) / t_end, "evals_per_s": evals / t_end, "seconds": t_end,
+                "max_inflight": st["max_inflight"], "loop_launches": st["loop_launches"]}
+
+    res = {"workload": f"serving: {n_requests} requests, Poisson {rate:g}/s, grids U{{512..4096}}^2, "
+                       f"halos log-U(50,5000), deflection or kappa/gamma/mu maps (chi2 requests not built)",
+           "precision": precision}
+    sat = run(arrivals)
+    res["at_rate"] = dict(sat, rate_per_s=rate, offered_over_capacity=rate / sat["requests_per_s"])
+    # a second pass at 70% of the measured capacity (the queue does not build up)
+    r70 = 0.7 * sat["requests_per_s"]
+    res["at_70pct_capacity"] = dict(run(arrivals * rate / r70), rate_per_s=r70)
+    # one plain FP64 call per request (host outputs, the reference's calling pattern)
+    idx = list(range(plain_sample))
+    t0 = time.perf_counter()
+    for i in idx:
+        k, n, c = reqs[i]
+        g = catalog.Grid.square(100., n)
+        if k == 0:
+            ctx.gradient_grid(dcats[c], g, precision="fp64", scale=D)
+        else:
+            ctx.hessian_maps(dcats[c], g, list(kinds_of[1]), precision="fp64", dlsds=D)
+    t = time.perf_counter() - t0
+    sample_evals = float(sum(reqs[i][1] ** 2 * pool[reqs[i][2]].n for i in idx))
+    # the sample's time scaled to all requests by halo x pixel evaluations
+    res["one_request_per_call_fp64"] = {"maps_per_s": nmaps / (t * evals / sample_evals),
+                                        "sample_requests": len(idx), "sample_s": t}
+    res["speedup_vs_one_request_per_call_fp64"] = sat["maps_per_s"] / res["one_request_per_call_fp64"]["maps_per_s"]
+    for c in dcats:
+        c.release()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32c"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp64", "fp32c"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -160,6 +341,11 @@ def main():
     ap.add_argument("--maps", default="all", choices=["all", "hessian", "potential"],
                     help="all = kappa/gamma1/gamma2/mu/psi (the workload); the others time one sum")
     ap.add_argument("--breakdown", action="store_true", help="also time the Hessian-only and potential-only passes")
+    ap.add_argument("--no-fp64-compare", action="store_true", help="skip timing LT_FP64 on the same workload")
+    ap.add_argument("--skip-batch", action="store_true", help="skip the posterior-batch workload")
+    ap.add_argument("--skip-serving", action="store_true", help="skip the serving workload")
+    ap.add_argument("--batch-sets", type=int, default=512)
+    ap.add_argument("--serving-requests", type=int, default=96)
     args = ap.parse_args()
     warmup = max(args.warmup, 3)
     rank, local_rank, world = dist_env()
@@ -254,6 +440,23 @@ def main():
             breakdown[label] = {"ms": dt * 1e3, "evals_per_s": g.npix * cat.n / dt}
     value = world * evals_step * args.steps / elapsed
 
+    # the same workload in LT_FP64 (the reference's FP64 arithmetic; Hessian bit-identical)
+    fp64_cmp = None
+    if rank == 0 and args.precision != "fp64" and not args.no_fp64_compare:
+        def step64():
+            ctx.lens_maps(dcat, g, precision="fp64", dlsds=D, out=outs, stream=stream, which=names)
+        step64()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k64 = 2
+        f0.record(stream)
+        for _ in range(k64):
+            step64()
+        f1.record(stream)
+        ctx.synchronize(stream)
+        t64 = f0.elapsed_time(f1) / 1e3 / k64
+        fp64_cmp = {"evals_per_s": evals_step / t64, "ms_per_step": t64 * 1e3, "steps": k64,
+                    "speedup_of_" + args.precision: (evals_step * args.steps / elapsed) / (evals_step / t64)}
+
     # end to end through the public API with host buffers: catalogue upload from host
     # arrays and the maps copied back into pinned host memory, every step
     e2e = None
@@ -307,8 +510,8 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                          "frac": achieved / peak_tflops if peak_tflops else None, "traffic": None,
-                         "kernel": f"lt::grid64_kernel<OP_HESS|OP_POT>" if args.precision == "fp64" else
-                         "lt::grid32c_kernel",
+                         "kernel": "lt::grid64_kernel<OP_HEX|OP_POT>" if args.precision == "fp64" else
+                         "lt::grid32c_kernel<OP_HESS|OP_POT>",
                          "flops_per_pair": fpp, "flop_convention": "weighted census, FMA-equivalents",
                          "peak_source": f"measured in-run: {pipe} FMA-chain kernel",
                          "hbm_writeback_gbs": out_bytes / per_launch / 1e9,
@@ -321,6 +524,13 @@ def main():
             line["breakdown"] = breakdown
         if cpu:
             line["cpu_baseline"] = cpu
+        if fp64_cmp:
+            line["fp64_same_workload"] = fp64_cmp
+        if world == 1 and not args.skip_batch:
+            line["posterior_batch"] = bench_posterior_batch(ctx, args.precision, steps=2, warmup=3,
+                                                            n_sets=args.batch_sets)
+        if world == 1 and not args.skip_serving:
+            line["serving"] = bench_serving(ctx, args.precision, n_requests=args.serving_requests)
         print(json.dumps(line))
     ctx.close()
     if world > 1:

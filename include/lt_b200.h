@@ -76,7 +76,11 @@ typedef enum {
     LT_MAP_GAMMA1 = 32,  /* (a - c) D/2                                                */
     LT_MAP_GAMMA2 = 33,  /* b D                                                        */
     LT_MAP_MU = 34,      /* 1/((1-kappa)^2 - gamma1^2 - gamma2^2), determinant in FP64 */
-    LT_MAP_MASS = 41     /* (a + c)/2 * mult (Kmap Hessian; mult per mass mode)        */
+    LT_MAP_MASS = 41,    /* (a + c)/2 * mult (Kmap Hessian; mult per mass mode)        */
+    /* batch and serving requests only (lt_request): */
+    LT_MAP_POTENTIAL = 51,    /* potential * scale                                     */
+    LT_MAP_DEFLECTION_X = 61, /* deflection x * scale (FP64 in every precision)        */
+    LT_MAP_DEFLECTION_Y = 62  /* deflection y * scale                                  */
 } lt_map_kind;
 
 #define LT_MAX_MAPS 8
@@ -170,6 +174,75 @@ lt_status lt_get_kernel_shape(const lt_context *ctx, int32_t precision, int32_t 
  * catalogue and keep the fastest in the context; *best_ms (may be NULL) gets its time. */
 lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision, int32_t sums, int32_t grid_n,
                       double *best_ms);
+
+/* ---- requests: batches and the serving loop ----------------------------------------
+ * A request is one grid of output planes over one uploaded catalogue: any mix of Hessian
+ * maps (lt_map_kind 0-41, with `dlsds` as D, `kmap` and `mult` as in lt_hessian_maps),
+ * the potential and the deflection (both multiplied by `scale`).  Results equal those of
+ * the single-grid calls in the same precision (LT_FP32C or LT_FP64) bit for bit.
+ * No counterpart in the reference, whose posterior driver makes one blocking map call
+ * per sample (utils/maps/main.cpp:432-587). */
+typedef struct {
+    const lt_catalog *cat;
+    lt_grid grid;
+    int32_t kmap;
+    double dlsds, mult, scale;
+    int32_t nmaps;
+    lt_map_request maps[LT_MAX_MAPS];
+} lt_request;
+
+typedef struct lt_batch lt_batch;
+
+/* Pack `nreqs` requests (device-pointer outputs) into a batch: one CUDA graph whose
+ * persistent kernel evaluates every request's pixel tiles, costliest requests first. */
+lt_status lt_batch_create(lt_context *ctx, const lt_request *reqs, int32_t nreqs, int32_t precision,
+                          lt_batch **batch);
+/* Replay the batch's graph on `stream` (asynchronous; lt_synchronize reports errors). */
+lt_status lt_batch_launch(lt_context *ctx, lt_batch *batch, void *stream);
+int32_t lt_batch_size(const lt_batch *batch);
+lt_status lt_batch_destroy(lt_context *ctx, lt_batch *batch);
+
+typedef struct lt_server lt_server;
+
+typedef struct {
+    int32_t precision;    /* LT_FP32C or LT_FP64                                          */
+    int32_t slots;        /* requests on the GPU at once (0: 64)                           */
+    int32_t window;       /* oldest requests served round-robin, tile by tile (0: 8)       */
+    int32_t idle_us;      /* idle time after which the persistent kernel leaves (0: 20000) */
+    size_t output_bytes;  /* HBM arena staging host-pointer outputs: the admission budget  */
+                          /* (0: 4 GiB)                                                    */
+} lt_server_config;
+
+typedef struct {
+    uint64_t submitted, admitted, completed, failed, loop_launches;
+    int32_t max_inflight, inflight, queued, loop_running;
+    size_t arena_bytes, arena_peak;
+    uint64_t device_published, device_head; /* the queue's counters as the device sees them */
+} lt_server_stats;
+
+/* Start a serving loop on the context.  While it runs, lt_catalog_release defers the
+ * release of catalogues until the context's last server is destroyed, and the context's
+ * other calls wait for the loop's kernel whenever it holds the SMs. */
+lt_status lt_server_create(lt_context *ctx, const lt_server_config *config, lt_server **server);
+/* Queue a request (host or device outputs; host outputs are staged in the arena and
+ * copied back, pinned host memory recommended).  Returns at once with a ticket;
+ * LT_ERR_BUDGET if the request's planes can never fit in the arena.  The server writes
+ * device outputs from its own stream: work that uses them must be complete at
+ * submission, and their contents are defined once the ticket completes. */
+lt_status lt_server_submit(lt_server *server, const lt_request *req, uint64_t *ticket);
+/* LT_OK when the ticket's results are in place, LT_ERR_NOT_READY before, or its error. */
+lt_status lt_server_poll(lt_server *server, uint64_t ticket);
+/* Block until the ticket completes or `timeout_s` passes (LT_ERR_NOT_READY). */
+lt_status lt_server_wait(lt_server *server, uint64_t ticket, double timeout_s);
+/* Milliseconds from submission to admission, admission to GPU completion, and
+ * submission to results in place. */
+lt_status lt_server_request_times(lt_server *server, uint64_t ticket, double *queued_ms, double *gpu_ms,
+                                  double *total_ms);
+/* Forget a completed ticket. */
+lt_status lt_server_release(lt_server *server, uint64_t ticket);
+lt_status lt_server_get_stats(lt_server *server, lt_server_stats *stats);
+/* Finish every submitted request, stop the loop and free the server. */
+lt_status lt_server_destroy(lt_server *server);
 
 /* Wait for the context's work on `stream` and report any status a kernel recorded
  * (e.g. LT_ERR_TIMEOUT from a bounded device-side wait).  Asynchronous (device-pointer)

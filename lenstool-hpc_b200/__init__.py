@@ -33,7 +33,9 @@ PRECISION = {"fp64": FP64, "fp32c": FP32C, "fp64fast": FP64_FAST, FP64: FP64, FP
 MAP = {"hess_a": 0, "hess_b": 1, "hess_c": 2, "hess_d": 3,
        "ampli1": 11, "ampli2": 12, "ampli3": 13, "ampli4": 14, "ampli5": 15, "ampli6": 16,
        "shear1": 21, "shear2": 22, "shear3": 23, "shear4": 24,
-       "kappa": 31, "gamma1": 32, "gamma2": 33, "mu": 34, "mass": 41}
+       "kappa": 31, "gamma1": 32, "gamma2": 33, "mu": 34, "mass": 41,
+       # batch and serving requests only
+       "potential": 51, "deflection_x": 61, "deflection_y": 62}
 MAX_MAPS = 8
 
 # physical constants of src/structure_hpc.hpp:62-73
@@ -68,6 +70,24 @@ class _MapReq(C.Structure):
     _fields_ = [("kind", C.c_int32), ("out", C.c_void_p)]
 
 
+class _Request(C.Structure):
+    _fields_ = [("cat", C.c_void_p), ("grid", _Grid), ("kmap", C.c_int32), ("dlsds", C.c_double),
+                ("mult", C.c_double), ("scale", C.c_double), ("nmaps", C.c_int32), ("maps", _MapReq * 8)]
+
+
+class _ServerConfig(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("slots", C.c_int32), ("window", C.c_int32), ("idle_us", C.c_int32),
+                ("output_bytes", C.c_size_t)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("failed", C.c_uint64), ("loop_launches", C.c_uint64), ("max_inflight", C.c_int32),
+                ("inflight", C.c_int32), ("queued", C.c_int32), ("loop_running", C.c_int32),
+                ("arena_bytes", C.c_size_t), ("arena_peak", C.c_size_t), ("device_published", C.c_uint64),
+                ("device_head", C.c_uint64)]
+
+
 class _Cosmo(C.Structure):
     _fields_ = [("model", C.c_int32), ("omegaM", C.c_double), ("omegaX", C.c_double), ("curvature", C.c_double),
                 ("wX", C.c_double), ("wa", C.c_double), ("H0", C.c_double)]
@@ -79,7 +99,10 @@ _LIB = None
 EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release", "lt_catalog_nhalos",
            "lt_gradient_grid", "lt_hessian_maps", "lt_potential_grid", "lt_lens_maps", "lt_synchronize",
            "lt_cosmo_distances", "lt_kernel_launch_count", "lt_status_string", "lt_last_error", "lt_abi_version",
-           "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_autotune", "lt_measure_fma_peak")
+           "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_autotune", "lt_measure_fma_peak",
+           "lt_batch_create", "lt_batch_launch", "lt_batch_size", "lt_batch_destroy", "lt_server_create",
+           "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
+           "lt_server_get_stats", "lt_server_destroy")
 SUMS = {"deflection": 1, "hessian": 2, "potential": 4, "lens": 6}
 
 
@@ -110,6 +133,18 @@ def load_library(path=None):
     L.lt_autotune.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
     L.lt_measure_fma_peak.argtypes = [C.c_int, C.c_int]
     L.lt_measure_fma_peak.restype = C.c_double
+    L.lt_batch_create.argtypes = [vp, C.POINTER(_Request), C.c_int32, C.c_int32, C.POINTER(vp)]
+    L.lt_batch_launch.argtypes = [vp, vp, vp]
+    L.lt_batch_size.argtypes = [vp]
+    L.lt_batch_destroy.argtypes = [vp, vp]
+    L.lt_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
+    L.lt_server_submit.argtypes = [vp, C.POINTER(_Request), C.POINTER(C.c_uint64)]
+    L.lt_server_poll.argtypes = [vp, C.c_uint64]
+    L.lt_server_wait.argtypes = [vp, C.c_uint64, C.c_double]
+    L.lt_server_request_times.argtypes = [vp, C.c_uint64, _dp, _dp, _dp]
+    L.lt_server_release.argtypes = [vp, C.c_uint64]
+    L.lt_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
+    L.lt_server_destroy.argtypes = [vp]
     L.lt_kernel_launch_count.restype = C.c_uint64
     L.lt_status_string.restype = C.c_char_p
     L.lt_status_string.argtypes = [C.c_int]
@@ -298,6 +333,135 @@ class Context:
 
     def synchronize(self, stream=None):
         self._check(self._lib.lt_synchronize(self.handle, _stream_handle(stream)), "lt_synchronize")
+
+    def batch(self, requests, precision="fp32c") -> "Batch":
+        """lt_batch_create: `requests` are Request objects with device outputs."""
+        reqs = list(requests)
+        arr = (_Request * len(reqs))(*[r.to_c(self) for r in reqs])
+        h = C.c_void_p()
+        st = self._lib.lt_batch_create(self.handle, arr, len(reqs), PRECISION[precision], C.byref(h))
+        self._check(st, "lt_batch_create")
+        return Batch(self, h, reqs)
+
+    def server(self, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0) -> "Server":
+        """lt_server_create: a continuous-batching serving loop on this context."""
+        return Server(self, precision, slots, window, idle_us, output_bytes)
+
+
+class Request:
+    """lt_request: one grid of output planes over one catalogue (batch / serving).
+
+    maps: {kind name or lt_map_kind: output array/tensor}."""
+
+    def __init__(self, cat, grid: Grid, maps, dlsds=1.0, kmap=False, mult=1.0, scale=1.0):
+        self.cat, self.grid, self.maps = cat, grid, dict(maps)
+        self.dlsds, self.kmap, self.mult, self.scale = dlsds, kmap, mult, scale
+        if not 1 <= len(self.maps) <= MAX_MAPS:
+            raise ValueError(f"a request has 1..{MAX_MAPS} maps")
+
+    def to_c(self, ctx: "Context") -> _Request:
+        cat = ctx._cat(self.cat)
+        self._cat_keep = cat
+        r = _Request()
+        r.cat = cat.handle
+        r.grid = _grid(self.grid)
+        r.kmap = int(bool(self.kmap))
+        r.dlsds, r.mult, r.scale = self.dlsds, self.mult, self.scale
+        r.nmaps = len(self.maps)
+        for i, (k, o) in enumerate(self.maps.items()):
+            r.maps[i] = _MapReq(MAP[k] if isinstance(k, str) else int(k), _ptr(o))
+        return r
+
+
+class Batch:
+    """lt_batch: requests evaluated by one graph-captured persistent launch."""
+
+    def __init__(self, ctx: Context, handle, requests):
+        self.ctx, self.handle, self.requests = ctx, handle, requests
+
+    def __len__(self):
+        return int(self.ctx._lib.lt_batch_size(self.handle))
+
+    def launch(self, stream=None):
+        self.ctx._check(self.ctx._lib.lt_batch_launch(self.ctx.handle, self.handle, _stream_handle(stream)),
+                        "lt_batch_launch")
+
+    def destroy(self):
+        if self.handle:
+            self.ctx._lib.lt_batch_destroy(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+
+class Server:
+    """lt_server: continuous batching of map requests on one context."""
+
+    def __init__(self, ctx: Context, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0):
+        self.ctx, self._lib = ctx, ctx._lib
+        cfg = _ServerConfig(PRECISION[precision], slots, window, idle_us, output_bytes)
+        h = C.c_void_p()
+        st = self._lib.lt_server_create(ctx.handle, C.byref(cfg), C.byref(h))
+        ctx._check(st, "lt_server_create")
+        self.handle = h
+        self._keep = {}
+
+    def submit(self, request: Request) -> int:
+        r = request.to_c(self.ctx)
+        t = C.c_uint64()
+        st = self._lib.lt_server_submit(self.handle, C.byref(r), C.byref(t))
+        self.ctx._check(st, "lt_server_submit")
+        self._keep[t.value] = request
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        st = self._lib.lt_server_poll(self.handle, ticket)
+        if st == 10:
+            return False
+        self.ctx._check(st, "lt_server_poll")
+        return True
+
+    def wait(self, ticket: int, timeout_s: float = 600.0):
+        st = self._lib.lt_server_wait(self.handle, ticket, timeout_s)
+        self.ctx._check(st, "lt_server_wait")
+
+    def times(self, ticket: int):
+        """(queued_ms, gpu_ms, total_ms) of a completed ticket."""
+        q, g, t = C.c_double(), C.c_double(), C.c_double()
+        st = self._lib.lt_server_request_times(self.handle, ticket, C.byref(q), C.byref(g), C.byref(t))
+        self.ctx._check(st, "lt_server_request_times")
+        return q.value, g.value, t.value
+
+    def release(self, ticket: int):
+        self._lib.lt_server_release(self.handle, ticket)
+        self._keep.pop(ticket, None)
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        self.ctx._check(self._lib.lt_server_get_stats(self.handle, C.byref(s)), "lt_server_get_stats")
+        return {f: getattr(s, f) for f, _ in _ServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            self._lib.lt_server_destroy(self.handle)
+            self.handle = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------------------

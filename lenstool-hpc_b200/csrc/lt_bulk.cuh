@@ -93,64 +93,90 @@ __device__ __forceinline__ double pixel_y(const GridArgs &a, int j)
     return __dadd_rn(a.ymin, __dmul_rn((double)(j + a.jstart), a.dy));
 }
 
+/* Round-to-nearest operations that the compiler may not fuse into FMAs: the map
+ * epilogues use them so that every kernel rounds a map exactly alike (and in the
+ * reference's C operation order), whatever the surrounding code. */
+namespace rn {
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double sqr(double a) { return __dsqrt_rn(a); }
+} // namespace rn
+
 /* Eigenvalues of [[A, B], [B, C]] (formeli_ampli, src/grid_map_ampli_GPU.cu:549-572). */
 __device__ __forceinline__ void eigen2(double A, double B, double C, double &lam, double &mu)
 {
-    double delta = (A - C) * (A - C) + 4. * B * B;
-    double e = sqrt(delta);
-    lam = .5 * (A + C + e);
-    mu = .5 * (A + C - e);
+    const double amc = rn::sub(A, C);
+    const double delta = rn::add(rn::mul(amc, amc), rn::mul(rn::mul(4., B), B));
+    const double e = rn::sqr(delta);
+    lam = rn::mul(.5, rn::add(rn::add(A, C), e));
+    mu = rn::mul(.5, rn::sub(rn::add(A, C), e));
 }
 
 /* Value of one output plane at one pixel from the pixel's sums (hyx: the Hessian's d
- * entry, equal to hxy up to rounding). */
+ * entry, equal to hxy up to rounding).  Formulas and operation order of the reference's
+ * map kernels: ampli src/grid_map_ampli_GPU.cu:329-547, shear src/grid_map_shear_GPU.cu:
+ * 208-369, mass src/grid_map_mass_GPU.cu:307-322. */
 __device__ __forceinline__ double map_value4(int kind, double gx, double gy, double hxx, double hyy, double hxy,
                                              double hyx, double psi, double D, double mult, double scale)
 {
-    double a = hxx, b = hxy, c = hyy;
+    using namespace rn;
+    const double a = hxx, b = hxy, c = hyy;
     double lam, mu;
     switch (kind) {
     case LT_MAP_HESS_A: return a;
     case LT_MAP_HESS_B: return b;
     case LT_MAP_HESS_C: return c;
     case LT_MAP_HESS_D: return hyx;
-    case LT_MAP_AMPLI1: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return 1. / (lam * mu);
-    case LT_MAP_AMPLI2: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return 1. / fabs(lam * mu);
-    case LT_MAP_AMPLI3: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return -2.5 * log10(fabs(lam * mu));
+    case LT_MAP_AMPLI1:
+        eigen2(sub(1., mul(a, D)), -mul(b, D), sub(1., mul(c, D)), lam, mu);
+        return div(1., mul(lam, mu));
+    case LT_MAP_AMPLI2:
+        eigen2(sub(1., mul(a, D)), -mul(b, D), sub(1., mul(c, D)), lam, mu);
+        return div(1., fabs(mul(lam, mu)));
+    case LT_MAP_AMPLI3:
+        eigen2(sub(1., mul(a, D)), -mul(b, D), sub(1., mul(c, D)), lam, mu);
+        return mul(-2.5, log10(fabs(mul(lam, mu))));
     case LT_MAP_AMPLI4: {
-        double k = (a + c) * D / 2.;
-        double g1 = (a - c) * D / 2.;
-        double g2 = b * D;
-        double g = sqrt(g1 * g1 + g2 * g2);
-        double gp = g / (1 - k);
-        return (1 - k) * (1 + gp * gp) / (1 - gp * gp);
+        const double k = div(mul(add(a, c), D), 2.);
+        const double g1 = div(mul(sub(a, c), D), 2.);
+        const double g2 = mul(b, D);
+        const double g = sqr(add(mul(g1, g1), mul(g2, g2)));
+        const double gp = div(g, sub(1., k));
+        const double gp2 = mul(gp, gp);
+        return div(mul(sub(1., k), add(1., gp2)), sub(1., gp2));
     }
-    case LT_MAP_AMPLI5: return (a + c) / 2.;
+    case LT_MAP_AMPLI5: return div(add(a, c), 2.);
     case LT_MAP_AMPLI6: {
-        double g1 = (a - c) / 2.;
-        return sqrt(g1 * g1 + b * b);
+        const double g1 = div(sub(a, c), 2.);
+        return sqr(add(mul(g1, g1), mul(b, b)));
     }
-    case LT_MAP_SHEAR1: eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu); return (lam - mu) / 2.;
+    case LT_MAP_SHEAR1:
+        eigen2(sub(1., mul(a, D)), -mul(b, D), sub(1., mul(c, D)), lam, mu);
+        return div(sub(lam, mu), 2.);
     case LT_MAP_SHEAR2: {
-        eigen2(1. - a * D, -b * D, 1. - c * D, lam, mu);
-        double q = lam / mu;
-        return fabs((q * q - 1.) / (q * q + 1.));
+        eigen2(sub(1., mul(a, D)), -mul(b, D), sub(1., mul(c, D)), lam, mu);
+        const double q = div(lam, mu);
+        const double q2 = mul(q, q);
+        return fabs(div(sub(q2, 1.), add(q2, 1.)));
     }
     case LT_MAP_SHEAR3:
-    case LT_MAP_GAMMA1: return (a - c) * D / 2.;
+    case LT_MAP_GAMMA1: return div(mul(sub(a, c), D), 2.);
     case LT_MAP_SHEAR4:
-    case LT_MAP_GAMMA2: return b * D;
-    case LT_MAP_KAPPA: return (a + c) * D / 2.;
+    case LT_MAP_GAMMA2: return mul(b, D);
+    case LT_MAP_KAPPA: return div(mul(add(a, c), D), 2.);
     case LT_MAP_MU: {
-        double k = (a + c) * D / 2.;
-        double g1 = (a - c) * D / 2.;
-        double g2 = b * D;
-        return 1. / ((1. - k) * (1. - k) - g1 * g1 - g2 * g2);
+        const double k = div(mul(add(a, c), D), 2.);
+        const double g1 = div(mul(sub(a, c), D), 2.);
+        const double g2 = mul(b, D);
+        const double omk = sub(1., k);
+        return div(1., sub(sub(mul(omk, omk), mul(g1, g1)), mul(g2, g2)));
     }
-    case LT_MAP_MASS: return (a + c) * 0.5 * mult;
-    case KIND_GRAD_X: return gx * scale;
-    case KIND_GRAD_Y: return gy * scale;
-    case KIND_POT: return psi * scale;
+    case LT_MAP_MASS: return mul(mul(add(a, c), 0.5), mult);
+    case KIND_GRAD_X: return mul(gx, scale);
+    case KIND_GRAD_Y: return mul(gy, scale);
+    case KIND_POT: return mul(psi, scale);
     default: return 0.;
     }
 }

@@ -213,6 +213,18 @@ std::vector<lt_chunk> lt::make_chunks(const int32_t *type, int n, int max_chunk,
     return ch;
 }
 
+/* (called with or without ctx->mu held: lt_catalog_upload releases a half-built
+ * catalogue under the lock) */
+void lt::free_catalog(lt_context *ctx, lt_catalog *cat)
+{
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    dev_free(ctx, cat->recs, sizeof(lt_rec64) * (size_t)cat->nhalos);
+    dev_free(ctx, cat->chunks, sizeof(lt_chunk) * (size_t)(cat->nchunks + cat->nchunks_k));
+    dev_free(ctx, cat->aux, cat->aux_bytes);
+    delete cat;
+}
+
 /* ------------------------------------------------------------------- API ---- */
 
 extern "C" {
@@ -261,12 +273,13 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
      * 1024^2 x 1000 halos; lt_autotune refines them for a given catalogue */
     for (int p = 0; p < 3; p++)
         for (int o = 0; o < 8; o++) ctx->shape[p][o] = LT_SHAPE(2, 1);
-    ctx->shape[LT_FP64][OP_HESS] = LT_SHAPE(1, 2);
-    ctx->shape[LT_FP64][OP_POT] = LT_SHAPE(1, 1);
+    ctx->shape[LT_FP64][OP_HESS] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP64][OP_POT] = LT_SHAPE(1, 2);
     ctx->shape[LT_FP64][OP_HESS | OP_POT] = LT_SHAPE(1, 2);
     ctx->shape[LT_FP64][OP_GRAD] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP64_FAST][OP_POT] = LT_SHAPE(1, 1);
-    ctx->shape[LT_FP64_FAST][OP_HESS | OP_POT] = LT_SHAPE(1, 1);
+    ctx->shape[LT_FP64_FAST][OP_HESS] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP64_FAST][OP_POT] = LT_SHAPE(1, 2);
+    ctx->shape[LT_FP64_FAST][OP_HESS | OP_POT] = LT_SHAPE(1, 2);
     ctx->shape[LT_FP64_FAST][OP_GRAD] = LT_SHAPE(2, 2);
     ctx->shape[LT_FP32C][OP_HESS] = LT_SHAPE(2, 2);
     ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE(2, 2);
@@ -349,11 +362,8 @@ lt_status lt_catalog_release(lt_context *ctx, lt_catalog *cat)
 {
     if (!ctx || !cat) return LT_ERR_INVALID_ARGUMENT;
     cudaSetDevice(ctx->device);
-    cudaDeviceSynchronize();
-    dev_free(ctx, cat->recs, sizeof(lt_rec64) * (size_t)cat->nhalos);
-    dev_free(ctx, cat->chunks, sizeof(lt_chunk) * (size_t)(cat->nchunks + cat->nchunks_k));
-    dev_free(ctx, cat->aux, cat->aux_bytes);
-    delete cat;
+    if (defer_release(ctx, cat)) return LT_OK;
+    free_catalog(ctx, cat);
     return LT_OK;
 }
 
@@ -380,7 +390,7 @@ lt_status lt_synchronize(lt_context *ctx, void *stream)
 
 /* ------------------------------------------------------------- grid calls ---- */
 
-static bool grid_ok(const lt_grid *g)
+bool lt::grid_ok(const lt_grid *g)
 {
     return g && g->nx > 0 && g->ny > 0 && std::isfinite(g->xmin) && std::isfinite(g->ymin) &&
            std::isfinite(g->dx) && std::isfinite(g->dy) && (long)g->nx * g->ny <= (1L << 31);
@@ -490,11 +500,15 @@ lt_status lt_gradient_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid
     return run_grid(ctx, cat, grid, precision, OP_GRAD, 0, 1.0, 1.0, scale, 2, kinds, outs, stream);
 }
 
-static bool hess_kind_ok(int k)
+} /* extern "C" */
+
+bool lt::hess_kind_ok(int k)
 {
     return (k >= LT_MAP_HESS_A && k <= LT_MAP_HESS_D) || (k >= LT_MAP_AMPLI1 && k <= LT_MAP_AMPLI6) ||
            (k >= LT_MAP_SHEAR1 && k <= LT_MAP_SHEAR4) || (k >= LT_MAP_KAPPA && k <= LT_MAP_MU) || k == LT_MAP_MASS;
 }
+
+extern "C" {
 
 lt_status lt_hessian_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t precision,
                           int32_t kmap, double dlsds, double mult, const lt_map_request *maps, int32_t nmaps,

@@ -24,19 +24,9 @@
 
 #include "lt_bulk.cuh"
 #include "lt_internal.h"
-#include "lt_profiles32.cuh"
-#include "lt_profiles64.cuh"
+#include "lt_eval.cuh"
 
 namespace lt {
-
-/* FP32C catalogue: FP32 records + a chunk list over both record kinds
- * (chunk.pad = 1: FP32 records of recs32, 0: FP64 records of recs64). */
-struct Fp32cCatalog {
-    lt_rec32 *recs32;
-    lt_chunk *chunks;
-    int32_t nchunks;
-    int32_t n32;
-};
 
 static const double kTau = 0.1;        /* FP64 where b0 / (2 r) > kTau                */
 /* FP64 within (kSingFrac + kSingEps e) rcut of the singular point: the FP32 forms lose
@@ -44,7 +34,7 @@ static const double kTau = 0.1;        /* FP64 where b0 / (2 r) > kTau          
 static const double kSingFrac = 0.3;
 static const double kSingEps = 1.5;
 static const double kCoreFrac = 3.0;   /* FP64 within 3 rcore of the centre           */
-static const double kMuFlag = 2.5;     /* recompute pixels with |mu| above this (error ~ mu^2) */
+static const double kMuFlag = LT_FP32C_MU_FLAG; /* recompute pixels with |mu| above this (error ~ mu^2) */
 
 static bool needs_fp64_always(const lt_rec64 &r, int type)
 {
@@ -190,84 +180,6 @@ struct C32Args {
     double mu_flag;
 };
 
-template <int P>
-struct Acc32 {
-    double hxx[P], hyy[P], hxy[P], psi[P]; /* FP64 terms, sky frame */
-    float ks[P], kc[P], g1s[P], g1c[P], g2s[P], g2c[P], ps[P], pc[P]; /* Kahan sums of FP32 terms */
-};
-
-template <int OP, int P, int TYPE>
-__device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, const double (&px)[P], double py, int kmap,
-                                             Acc32<P> &acc)
-{
-#pragma unroll 1
-    for (int h = 0; h < count; h++) {
-        const lt_rec64 &r = recs[h];
-        const double w = kmap ? r.w : 1.0;
-#pragma unroll
-        for (int k = 0; k < P; k++) {
-            if (OP & OP_HESS) {
-                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
-                hess_pair<TYPE>(r, px[k], py, w, hh);
-                acc.hxx[k] = hh.xx;
-                acc.hyy[k] = hh.yy;
-                acc.hxy[k] = hh.xy;
-            }
-            if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
-        }
-    }
-}
-
-template <int OP, int P, int TYPE>
-__device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec64 *recs64, int count,
-                                             const double (&px)[P], double py, int kmap, Acc32<P> &acc)
-{
-#pragma unroll 1
-    for (int h = 0; h < count; h++) {
-        const lt_rec32 &r = recs[h];
-        float u[P], v[P];
-        bool near = false;
-        const float ty = (float)(py - r.y0);
-#pragma unroll
-        for (int k = 0; k < P; k++) {
-            const float tx = (float)(px[k] - r.x0);
-            u[k] = tx * r.cs + ty * r.sn;
-            v[k] = ty * r.cs - tx * r.sn;
-            const float rr = u[k] * u[k] + v[k] * v[k];
-            const float dv = v[k] - r.singv;
-            near |= (rr < r.rnear2) | (u[k] * u[k] + dv * dv < r.sing_r2) | (rr < r.core_r2);
-        }
-        if (OP & OP_POT) {
-#pragma unroll
-            for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
-        }
-        if (!(OP & OP_HESS)) continue;
-        if (__any_sync(0xffffffffu, near)) {
-            const lt_rec64 &r64 = recs64[r.idx64];
-            const double w = kmap ? r64.w : 1.0;
-#pragma unroll
-            for (int k = 0; k < P; k++) {
-                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
-                hess_pair<TYPE>(r64, px[k], py, w, hh);
-                acc.hxx[k] = hh.xx;
-                acc.hyy[k] = hh.yy;
-                acc.hxy[k] = hh.xy;
-            }
-        } else {
-            const float w = kmap ? r.w : 1.0f;
-#pragma unroll
-            for (int k = 0; k < P; k++) {
-                KG32 t = hess32<TYPE>(r, u[k], v[k]);
-                const float g1 = t.g1 * r.c2t - t.g2 * r.s2t;
-                const float g2 = t.g1 * r.s2t + t.g2 * r.c2t;
-                kahan_add(acc.ks[k], acc.kc[k], w * t.k);
-                kahan_add(acc.g1s[k], acc.g1c[k], w * g1);
-                kahan_add(acc.g2s[k], acc.g2c[k], w * g2);
-            }
-        }
-    }
-}
-
 template <int OP, int P, int MINB>
 __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args A)
 {
@@ -368,15 +280,8 @@ __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args
             bool flag[P];
 #pragma unroll
             for (int k = 0; k < P; k++) {
-                const double kap = 0.5 * (acc.hxx[k] + acc.hyy[k]) + ((double)acc.ks[k] - (double)acc.kc[k]);
-                const double g1 = 0.5 * (acc.hxx[k] - acc.hyy[k]) + ((double)acc.g1s[k] - (double)acc.g1c[k]);
-                const double g2 = acc.hxy[k] + ((double)acc.g2s[k] - (double)acc.g2c[k]);
-                hxx[k] = kap + g1;
-                hyy[k] = kap - g1;
-                hxy[k] = g2;
-                psi[k] = acc.psi[k] + ((double)acc.ps[k] - (double)acc.pc[k]);
-                const double kd = kap * a.D, g1d = g1 * a.D, g2d = g2 * a.D;
-                const double det = (1. - kd) * (1. - kd) - g1d * g1d - g2d * g2d;
+                double det;
+                fp32c_total(acc, k, a.D, hxx[k], hyy[k], hxy[k], psi[k], det);
                 flag[k] = (OP & OP_HESS) && !(fabs(det) * A.mu_flag >= 1.0);
             }
             const bool full = a.vec_ok && (ix + P <= a.nx);
@@ -429,7 +334,7 @@ static void (*pick_kernel32(int op, int shape))(const C32Args)
 }
 
 /* maps whose value depends on the Jacobian determinant (amplified near critical curves) */
-static bool det_sensitive(int kind)
+bool det_sensitive(int kind)
 {
     return kind == LT_MAP_MU || kind == LT_MAP_AMPLI1 || kind == LT_MAP_AMPLI2 || kind == LT_MAP_AMPLI3 ||
            kind == LT_MAP_AMPLI4 || kind == LT_MAP_SHEAR2;
@@ -493,9 +398,5 @@ int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, vo
     return err;
 }
 
-void destroy_extensions(lt_context *ctx)
-{
-    (void)ctx;
-}
 
 } // namespace lt

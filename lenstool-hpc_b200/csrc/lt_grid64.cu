@@ -16,66 +16,11 @@
 #include <cuda_runtime.h>
 #include "lt_bulk.cuh"
 #include "lt_internal.h"
-#include "lt_profiles64.cuh"
+#include "lt_eval.cuh"
 
 namespace lt {
 
 constexpr int kThreads = 256;
-
-template <int OP, int P>
-struct Acc64 {
-    double gx[P], gy[P], hxx[P], hyy[P], hxy[P], psi[P];
-    ex::Mat run[P], tot[P]; /* OP_HEX: the reference's per-run and total sums */
-};
-
-template <int OP, int P, int TYPE>
-__device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, const double (&px)[P], double py,
-                                             int kmap, Acc64<OP, P> &acc)
-{
-#pragma unroll 1
-    for (int h = 0; h < count; h++) {
-        const lt_rec64 &r = recs[h];
-        double w = kmap ? r.w : 1.0;
-#pragma unroll
-        for (int k = 0; k < P; k++) {
-            if (OP & OP_GRAD) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
-            if (OP & OP_HESS) {
-                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
-                hess_pair<TYPE>(r, px[k], py, w, hh);
-                acc.hxx[k] = hh.xx;
-                acc.hyy[k] = hh.yy;
-                acc.hxy[k] = hh.xy;
-            }
-            if (OP & OP_HEX) ex::hess_pair<TYPE>(r, px[k], py, acc.run[k]);
-            if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
-        }
-    }
-}
-
-/* End of a run of the reference's dispatch (src/gradient2.cpp:240-251): the run's sum
- * joins the total, weighted by the run's dlsds for the Kmap
- * (src/gradient2_GPU.cu:503-507). */
-template <int OP, int P>
-__device__ __forceinline__ void close_run64(Acc64<OP, P> &acc, int kmap, double w)
-{
-#pragma unroll
-    for (int k = 0; k < P; k++) {
-        ex::Mat &t = acc.tot[k];
-        const ex::Mat &r = acc.run[k];
-        if (kmap) {
-            t.a = ex::A(t.a, ex::M(r.a, w));
-            t.b = ex::A(t.b, ex::M(r.b, w));
-            t.c = ex::A(t.c, ex::M(r.c, w));
-            t.d = ex::A(t.d, ex::M(r.d, w));
-        } else {
-            t.a = ex::A(t.a, r.a);
-            t.b = ex::A(t.b, r.b);
-            t.c = ex::A(t.c, r.c);
-            t.d = ex::A(t.d, r.d);
-        }
-        acc.run[k].a = acc.run[k].b = acc.run[k].c = acc.run[k].d = 0.;
-    }
-}
 
 template <int OP, int P, bool LIST, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a)

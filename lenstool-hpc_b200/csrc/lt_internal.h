@@ -41,7 +41,22 @@ struct lt_catalog {
     alignas(16) unsigned char aux_desc[64]; /* FP32C descriptor (host) */
 };
 
+struct lt_rec32;
+
+/* FP32C: pixels with |mu| above this are recomputed in FP64 (the FP32C error of mu grows
+ * as mu^2 near critical curves) */
+#define LT_FP32C_MU_FLAG 2.5
+
 namespace lt {
+
+/* FP32C catalogue (lt_catalog::aux_desc): FP32 records + a chunk list over both record
+ * kinds (chunk.pad & CHUNK_FP32: FP32 records of recs32, else FP64 records of recs64). */
+struct Fp32cCatalog {
+    lt_rec32 *recs32;
+    lt_chunk *chunks;
+    int32_t nchunks;
+    int32_t n32;
+};
 
 void count_launch(uint64_t n);
 void set_error(lt_context *ctx, const char *fmt, ...);
@@ -65,6 +80,17 @@ lt_status list_buffer(lt_context *ctx, long npix, int32_t **list, int32_t **coun
 /* FP32-compensated path (lt_grid32.cu) */
 lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat);
 int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, void *stream);
+/* true for map kinds whose value depends on the Jacobian determinant */
+bool det_sensitive(int kind);
+bool grid_ok(const lt_grid *g);
+bool hess_kind_ok(int kind);
+
+/* batches and the serving loop (lt_queue.cu) */
 void destroy_extensions(lt_context *ctx);
+/* true when the catalogue's memory must outlive a running serving loop: it is then
+ * released when the last server of the context is destroyed */
+bool defer_release(lt_context *ctx, lt_catalog *cat);
+/* free a catalogue's device memory (waits for the device) */
+void free_catalog(lt_context *ctx, lt_catalog *cat);
 
 } // namespace lt

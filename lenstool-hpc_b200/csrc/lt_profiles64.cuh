@@ -91,11 +91,19 @@ struct Hess64 {
     double xx, yy, xy;
 };
 
-/* The three bracketed terms of mdci05 (didxre, didyre, didyim without the factor ci). */
+/* The three bracketed terms of mdci05 (didxre, didyre, didyim without the factor ci).
+ * With t1 = 2 sqrt(e) w - v/cx1 (the small factor of den1 near the removable singular
+ * point u = 0, v = 2 r sqrt(e)), the numerators factor exactly:
+ *   didxre: cx1 (2 sqrt(e) u^2/((1+e)^2 w) - t1)
+ *   didyre: u (2 sqrt(e) v cx1/((1-e)^2 w) - 1)
+ *   didyim: t1 (1/cx1 - 2 sqrt(e) v/((1-e)^2 w))
+ * (for didyim, 4e = (2 sqrt(e))^2 turns the reference's four terms into the product), so
+ * numerator and denominator share one rounded t1 and the numerators cancel no digits. */
 __device__ __forceinline__ void mdci05_terms(const lt_rec64 &h, double u, double uu, double v, double vv,
                                              double vq, double rem2, double r2, double tsr, double &X, double &Y,
                                              double &Z)
 {
+    (void)vv;
     double wrem = sqrt(r2 + rem2);
     double iw = 1.0 / wrem;
     double t1 = h.sqe2 * wrem - vq;
@@ -104,10 +112,10 @@ __device__ __forceinline__ void mdci05_terms(const lt_rec64 &h, double u, double
     double den2 = uu + num2 * num2;
     double i1 = 1.0 / den1;
     double i2 = 1.0 / den2;
-    X = h.cx1 * (h.sqe2 * uu * h.cxro_inv * iw - h.sqe2 * wrem + vq) * i1 + num2 * i2;
-    Y = (h.sqe2 * u * v * h.cx1 * h.cyro_inv * iw - u) * i1 + u * i2;
-    Z = (h.sqe2 * wrem * h.cx1inv - vq * h.cx1inv - h.k4 * v * h.cyro_inv + h.sqe2 * vv * h.cyro_inv * iw * h.cx1inv) * i1 -
-        num2 * i2;
+    double sv = h.sqe2 * v * h.cyro_inv * iw;
+    X = h.cx1 * (h.sqe2 * uu * h.cxro_inv * iw - t1) * i1 + num2 * i2;
+    Y = u * (sv * h.cx1 - 1.0) * i1 + u * i2;
+    Z = t1 * (h.cx1inv - sv) * i1 - num2 * i2;
 }
 
 /* H = R^T H' R for the symmetric halo-frame Hessian H' = [[a, b], [b, c]]; the

@@ -1,0 +1,67 @@
+/*
+ * lt_queue.h -- device layout of the work queue shared by the batch and serving entry
+ * points (lt_batch.cpp, lt_server.cpp) and the persistent kernel (lt_queue.cu).
+ */
+#pragma once
+#include <stdint.h>
+
+#include <cuda_runtime.h>
+
+#include "lt_grid.cuh"
+
+struct lt_rec32;
+
+namespace lt {
+
+/* kernel modes: FP32C tiles (P = 2), or the LT_FP64 tiles with the reference-order
+ * Hessian (P per request) */
+enum { QMODE_C32 = 0, QMODE_EXACT = 1 };
+
+/* One request: one grid of output planes over one catalogue. */
+struct alignas(16) QItem {
+    GridArgs g;                 /* FP64 records and chunk list (the Kmap list when kmap),
+                                   geometry (tiles_x, ntiles for this request's P),
+                                   outputs, D, mult, scale, status */
+    const lt_rec32 *recs32;     /* FP32C records */
+    const lt_chunk *chunks32;   /* FP32C chunk list (FP32 and FP64-class chunks) */
+    int32_t nchunks32;
+    int32_t op;                 /* OP_GRAD | OP_HESS | OP_POT */
+    int32_t ntiles;
+    uint32_t seq;               /* request sequence number (low 32 bits) */
+    int32_t ppt;                /* pixels per thread of the tiles (QMODE_EXACT) */
+    int32_t pad0;
+    double mu_flag;             /* FP32C: recompute pixels with |mu| > mu_flag in FP64 */
+    uint32_t *host_flag;        /* mapped host word set to seq + 1 on completion, or null */
+    int64_t pad1;
+};
+static_assert(sizeof(QItem) % 16 == 0, "QItem is copied in 16-byte units");
+
+struct alignas(16) QSlot {
+    QItem item;
+    unsigned long long ctr;     /* (seq << 32) | next tile to claim */
+    unsigned int done;          /* tiles completed */
+    unsigned int pad;
+};
+
+struct alignas(16) QState {
+    unsigned long long published; /* requests published (host-written) */
+    unsigned long long head;       /* oldest request that may have unclaimed tiles */
+    unsigned long long rotor;      /* round-robin counter over the window */
+    int32_t stop;                  /* leave when no published request has work */
+    int32_t pad;
+};
+
+struct QArgs {
+    QSlot *slots;
+    QState *state;
+    int32_t nslots;
+    int32_t window;                /* requests served round-robin (1: first come, first served) */
+    int32_t idle_polls;            /* polls of ~1 us before an idle CTA leaves */
+    int32_t *status;               /* device status word (LT_ERR_TIMEOUT from a bounded wait) */
+};
+
+int queue_blocks(int mode, int num_sms);
+int launch_queue(int mode, const QArgs &q, int blocks, cudaStream_t s);
+int launch_queue_reset(QSlot *slots, QState *state, int n, cudaStream_t s);
+
+} // namespace lt
