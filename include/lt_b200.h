@@ -244,6 +244,23 @@ lt_status lt_server_get_stats(lt_server *server, lt_server_stats *stats);
 /* Finish every submitted request, stop the loop and free the server. */
 lt_status lt_server_destroy(lt_server *server);
 
+/* ---- Hessian maps without allocation ------------------------------------------------
+ * lt_hessian_maps in LT_FP32C with device outputs, for callers that must not allocate
+ * device memory during a call (a process running under a fixed device-memory plan, or a
+ * timed loop that must not meet cudaMalloc's implicit synchronisation): the list of
+ * pixels recomputed in FP64 lives in a static 16 MiB device array instead of a context
+ * buffer grown with cudaMalloc, and the call allocates nothing.  The list's length word
+ * must start at zero; the call zeroes it on `stream` itself.  Limits: grids of at most
+ * 2048 x 2048 pixels (larger: LT_ERR_INVALID_ARGUMENT), device outputs only, and one array
+ * per process and device, so calls that overlap in time race on it and must be
+ * serialised by the caller.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress, return code checked) and loads the module's data there; make
+ * that first call before any stream capture that includes this call.  No counterpart in
+ * the reference. */
+lt_status lt_hessian_maps_noalloc(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t kmap,
+                                  double dlsds, double mult, const lt_map_request *maps, int32_t nmaps,
+                                  void *stream);
+
 /* Wait for the context's work on `stream` and report any status a kernel recorded
  * (e.g. LT_ERR_TIMEOUT from a bounded device-side wait).  Asynchronous (device-pointer)
  * calls report such errors here. */

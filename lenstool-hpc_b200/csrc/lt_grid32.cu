@@ -398,5 +398,54 @@ int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, vo
     return err;
 }
 
+/* launch_fp32c for the Hessian maps with a caller-provided recomputation list: `list`
+ * holds up to `cap` pixel indices and `count` its length word, which this function
+ * zeroes on `stream` before pass 1.  Nothing is allocated. */
+int launch_fp32c_with_list(lt_context *ctx, const lt_catalog *cat, GridArgs &a, int32_t *list, int32_t *count,
+                           int32_t cap, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    const Fp32cCatalog &fc = *reinterpret_cast<const Fp32cCatalog *>(&cat->aux_desc);
+    C32Args A;
+    memset(&A, 0, sizeof(A));
+    A.g = a;
+    bool det = false;
+    for (int o = 0; o < a.nout; o++) det |= det_sensitive(a.kinds[o]);
+    const int shape = ctx->shape[LT_FP32C][OP_HESS];
+    const int ppt = (shape & 15) == 1 ? 1 : 2;
+    A.g.tiles_x = (a.nx + 32 * ppt - 1) / (32 * ppt);
+    A.g.ntiles = A.g.tiles_x * ((a.ny + 7) / 8);
+    A.recs32 = fc.recs32;
+    A.chunks = fc.chunks;
+    A.nchunks = fc.nchunks;
+    A.mu_flag = det ? kMuFlag : 0.0;
+    if (det) {
+        if ((long)a.nx * a.ny > (long)cap) return (int)cudaErrorInvalidValue;
+        A.list = list;
+        A.list_count = count;
+        A.list_cap = cap;
+        cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int32_t), s);
+        if (e != cudaSuccess) return (int)e;
+    }
+    const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
+    void (*kern)(const C32Args) = pick_kernel32(OP_HESS, shape);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads32, smem);
+    if (per_sm < 1) per_sm = 1;
+    int blocks = ctx->num_sms * per_sm;
+    if (blocks > A.g.ntiles) blocks = A.g.ntiles;
+    kern<<<blocks, kThreads32, smem, s>>>(A);
+    count_launch(1);
+    int err = (int)cudaGetLastError();
+    if (err != cudaSuccess || !det) return err;
+    GridArgs r = A.g;
+    r.list = A.list;
+    r.list_count = A.list_count;
+    r.list_cap = A.list_cap;
+    err = launch_grid64_list(OP_HESS, r, ctx->num_sms, stream);
+    count_launch(1);
+    return err;
+}
+
 
 } // namespace lt
