@@ -2,12 +2,16 @@
 
 One step = kappa, gamma1, gamma2, mu and the potential (x D_LS/D_OS) of the 4096^2 grid
 over 300"x300" for the seeded 1000-halo catalogue (4 cluster-scale + 996 galaxy-scale
-cut-dPIE halos), computed by the fused lens-maps kernel.  Metric: halo x pixel
-evaluations per second, counting the Hessian and the potential sum once each per
-(halo, pixel) pair.
+cut-dPIE halos), computed by the fused lens-maps kernel (LT_FP32C by default).  Metric:
+halo x pixel evaluations per second, counting the Hessian and the potential sum once each
+per (halo, pixel) pair.  The same JSON line also carries LT_FP64 on the same step, the
+posterior-batch workload (maps/s against one map call per set), the serving workload
+(p50/p99 latency, maps/s against one plain call per request) and the delensing + chi2
+workload (models/s against the reference's CPU code).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp32c|fp64]
-                  [--impl ours|reference]
+                  [--impl ours|reference] [--skip-batch] [--skip-serving] [--skip-chi2]
+                  [--only-batch --batch-sets N]
 
 --impl reference times the reference's own CPU code (oracle/_ref: gradient2_grid_CPU and
 the reference potential kernel compiled for the host) on all host cores, on a bounded
@@ -39,6 +43,10 @@ METRIC = "halo x pixel evals/s (Hessian + potential, lens maps kappa/gamma1/gamm
 # log = atan2 = 20): dPIE Hessian 182 (src/gradient2.cpp:92-167, :54-83) + dPIE potential
 # 760 (src/potential_GPU.cu:47-116 with src/lt_math_GPU.cuh)
 FLOPS_PER_PAIR = 182 + 760
+# DRAM bytes (read + write) of one launch of the default step's dominant kernel
+# (grid32c_kernel<OP_HESS|OP_POT>, FP32C, 4096^2 x 1000 halos), from a single-pass ncu
+# capture of this bench's own launch: profiles/launches_lens_maps_fp32c_1000h_4096.md
+TRAFFIC_FP32C_LENS_4096 = 28741376 + 642056192
 
 
 def _package():
@@ -221,27 +229,34 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
         res["e2e"] = {"skipped": f"host memory available {host_free / 1e9:.0f} GB < 3x the maps"}
         e2e = False
     if e2e:
-        # end to end through the public API: the sets' catalogues uploaded from host arrays,
-        # the batch built (graph captured), launched, and every map copied to host memory
-        host = [{k: torch.empty((int(n), int(n)), dtype=torch.float64).numpy() for k in kinds} for n in sizes]
-        t0 = time.perf_counter()
-        cats2 = [ctx.upload(c) for c in sets]
-        b2 = ctx.batch([lt.Request(c, grids[int(n)], o, dlsds=D) for c, n, o in zip(cats2, sizes, outs)],
-                       precision=precision)
-        b2.launch(stream)
-        ctx.synchronize(stream)
-        for o, h in zip(outs, host):
-            for k in kinds:
-                torch.from_numpy(h[k]).copy_(o[k])
-        b2.destroy()
+        # end to end through the public API: every set's catalogue uploaded from host arrays
+        # and every map delivered to (pinned) host memory, through the serving loop, which
+        # copies finished sets out while later ones compute.  The host buffers and the
+        # server are set up outside the timed region.
+        batch.destroy()
+        batch = None
+        host = [{k: torch.empty((int(n), int(n)), dtype=torch.float64, pin_memory=True) for k in kinds}
+                for n in sizes]
+        with ctx.server(precision=precision, slots=64, window=8, output_bytes=8 << 30) as srv:
+            srv.wait(srv.submit(lt.Request(cats[0], grids[512], {"kappa": host[0]["kappa"][:512, :512].contiguous()},
+                                           dlsds=D)))
+            t0 = time.perf_counter()
+            cats2 = [ctx.upload(c) for c in sets]
+            tickets = [srv.submit(lt.Request(c, grids[int(n)], h, dlsds=D)) for c, n, h in zip(cats2, sizes, host)]
+            for t in tickets:
+                srv.wait(t, 3600.)
+            te = time.perf_counter() - t0
+            for t in tickets:
+                srv.release(t)
         for c in cats2:
             c.release()
-        te = time.perf_counter() - t0
         res["e2e"] = {"maps_per_s": 2 * n_sets / te, "h2d_bytes_per_step": n_sets * base.n * (192 + 160),
                       "d2h_bytes_per_step": int(2 * 8 * evals / base.n),
-                      "note": "upload of every set's catalogue + batch build + launch + maps to pageable host"}
+                      "note": "upload of every set's catalogue + every set served (lt_server) with its maps "
+                              "copied to pinned host memory while later sets compute"}
         res["e2e"]["speedup_vs_one_map_per_call_fp64"] = res["e2e"]["maps_per_s"] / plain["fp64"]["maps_per_s"]
-    batch.destroy()
+    if batch is not None:
+        batch.destroy()
     for c in cats:
         c.release()
     return res
@@ -328,6 +343,54 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=8, see
     return res
 
 
+def bench_chi2(ctx, n_models=64, n=2048, nsys=40, seed=20261203 + 3, cpu=True):
+    """Delensing + chi2 workload: perturbed models (5% Gaussian, seeded) of the 200-halo
+    catalogue against 40 multiple-image systems with 3-5 images each, generated by
+    forward ray-shooting of seeded sources through the true model (delensing on a 2048^2
+    grid) plus 0.05" Gaussian noise; per model a 2048^2 deflection grid, barycentric
+    delensing and the FP64 chi2 (lt_chi2_batch).  A sample of n_models models is timed
+    (the 4096-model batch takes 4096 / models_per_s)."""
+    lt = _package()
+    from lenstool_hpc_b200 import catalog
+    from lenstool_hpc_b200.images import generate_systems
+    frame = (-100., 100., -100., 100.)
+    base = catalog.cluster_galaxy_catalog(2, 198, 20261203)
+    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
+    D = dls / dos
+    dbase = ctx.upload(base)
+    ic = int(np.argmax(base.b0))
+    systems = generate_systems(lambda bx, by, dr: ctx.delense(dbase, frame, n, bx, by, dr), nsys, seed, dr=D,
+                               centre=(base.position_x[ic], base.position_y[ic]), source_radius=10.)
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    models = [ctx.upload(catalog.perturb_catalog(base, rng)) for _ in range(n_models)]
+    ctx.chi2(models[:2], frame, n, systems)  # warm-up
+    t0 = time.perf_counter()
+    chi, found = ctx.chi2(models, frame, n, systems)
+    dt = time.perf_counter() - t0
+    true_chi, _ = ctx.chi2(dbase, frame, n, systems)
+    res = {"workload": f"chi2_batch: {n_models} of 4096 perturbed models x {base.n} halos, {nsys} systems "
+                       f"({systems.nimages} images), {n}^2 delensing grid, FP64",
+           "models_per_s": n_models / dt, "ms_per_model": 1e3 * dt / n_models,
+           "seconds_for_4096_models": 4096 * dt / n_models, "deflection_evals_per_s": n_models * n * n * base.n / dt,
+           "chi2_true_model": true_chi, "chi2_median_perturbed": float(np.median(chi))}
+    if cpu:
+        try:
+            import oracle
+            ref = oracle.RefLib()
+            t0 = time.perf_counter()
+            r = ref.chi2(base, frame, n, systems.nimg, systems.x, systems.y, systems.dr)
+            tc = time.perf_counter() - t0
+            res["cpu_baseline"] = {"models_per_s": 1. / tc, "cores": os.cpu_count(), "kind": "reference",
+                                   "sample": f"1 model: gradient_grid_CPU ({os.cpu_count()} threads) + "
+                                             "delense_barycenter (1 thread, its serial order) + chi_computation",
+                                   "chi2_true_model": r["chi2"]}
+        except Exception as ex:
+            res["cpu_baseline"] = {"unavailable": str(ex)}
+    for m in models:
+        m.release()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,7 +407,10 @@ def main():
     ap.add_argument("--no-fp64-compare", action="store_true", help="skip timing LT_FP64 on the same workload")
     ap.add_argument("--skip-batch", action="store_true", help="skip the posterior-batch workload")
     ap.add_argument("--skip-serving", action="store_true", help="skip the serving workload")
+    ap.add_argument("--skip-chi2", action="store_true", help="skip the delensing + chi2 workload")
     ap.add_argument("--batch-sets", type=int, default=512)
+    ap.add_argument("--only-batch", action="store_true",
+                    help="run only the posterior-batch workload (--batch-sets sets, --steps launches) and print it")
     ap.add_argument("--serving-requests", type=int, default=96)
     args = ap.parse_args()
     warmup = max(args.warmup, 3)
@@ -372,6 +438,14 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     build.build()
+    if args.only_batch:
+        ctx = lt.Context(local_rank)
+        res = bench_posterior_batch(ctx, args.precision, steps=args.steps, warmup=warmup, n_sets=args.batch_sets,
+                                    e2e=not args.no_e2e)
+        if rank == 0:
+            print(json.dumps({"posterior_batch": res}))
+        ctx.close()
+        return 0
     cat, g = catalog.workload(WORKLOAD)
     if args.grid:
         g = catalog.Grid.square(150., args.grid)
@@ -509,7 +583,10 @@ def main():
                        "l2": "outputs 671 MB per step > 126 MB L2; catalogue 192 KB stays resident"},
             "gpu_launches": int(launches),
             "roofline": {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / peak_tflops if peak_tflops else None, "traffic": None,
+                         "frac": achieved / peak_tflops if peak_tflops else None,
+                         "traffic": TRAFFIC_FP32C_LENS_4096 if (args.precision == "fp32c" and args.maps == "all"
+                                                                and not args.grid) else None,
+                         "traffic_algorithmic": out_bytes,
                          "kernel": "lt::grid64_kernel<OP_HEX|OP_POT>" if args.precision == "fp64" else
                          "lt::grid32c_kernel<OP_HESS|OP_POT>",
                          "flops_per_pair": fpp, "flop_convention": "weighted census, FMA-equivalents",
@@ -531,6 +608,8 @@ def main():
                                                             n_sets=args.batch_sets)
         if world == 1 and not args.skip_serving:
             line["serving"] = bench_serving(ctx, args.precision, n_requests=args.serving_requests)
+        if world == 1 and not args.skip_chi2:
+            line["chi2_batch"] = bench_chi2(ctx, cpu=not args.no_cpu_baseline)
         print(json.dumps(line))
     ctx.close()
     if world > 1:

@@ -52,9 +52,9 @@ typedef enum {
  *          sequence (bit-identical to the reference CPU path), deflection and potential
  *          agree to <= 1e-12.
  * LT_FP32C: FP32 bulk with compensated accumulation and FP64 where FP32 loses digits.
- * LT_FP64_FAST: FP64 with reciprocals, FMA and shared sub-expressions; as accurate as
- *          LT_FP64 on average, but its rounding differs, so at the formula's
- *          ill-conditioned pixels it departs from the reference by up to ~1e-11. */
+ * LT_FP64_FAST: FP64 with reciprocals, FMA and shared sub-expressions; within 2e-12 of
+ *          the reference except at the formula's ill-conditioned pixels (within ~1e-3"
+ *          of each halo's removable singular points), where it departs by up to ~1e-11. */
 typedef enum { LT_FP64 = 0, LT_FP32C = 1, LT_FP64_FAST = 2 } lt_precision;
 
 /* Map kinds computed from the Hessian [[a, b], [d, c]] with D = dlsds (D_LS/D_OS).
@@ -79,7 +79,7 @@ typedef enum {
     LT_MAP_MASS = 41,    /* (a + c)/2 * mult (Kmap Hessian; mult per mass mode)        */
     /* batch and serving requests only (lt_request): */
     LT_MAP_POTENTIAL = 51,    /* potential * scale                                     */
-    LT_MAP_DEFLECTION_X = 61, /* deflection x * scale (FP64 in every precision)        */
+    LT_MAP_DEFLECTION_X = 61, /* deflection x * scale                                  */
     LT_MAP_DEFLECTION_Y = 62  /* deflection y * scale                                  */
 } lt_map_kind;
 
@@ -261,6 +261,49 @@ lt_status lt_hessian_maps_noalloc(lt_context *ctx, const lt_catalog *cat, const 
                                   double dlsds, double mult, const lt_map_request *maps, int32_t nmaps,
                                   void *stream);
 
+/* ---- strong-lensing chi2 by barycentric delensing -----------------------------------
+ * The reference's chi2 of a model (mychi_bruteforce_SOA_CPU_grid_gradient_barycentersource,
+ * src/chi_CPU_barycenter.cpp:58-287): the deflection grid over `frame` with n x n pixels
+ * (dx = (xmax - xmin)/(n - 1)), each system's source as the barycentre of its images
+ * mapped to the source plane, the predicted images of that source by delensing the grid's
+ * triangles (src/delense_CPU.cpp:6-140), and the link of predicted to observed images
+ * with chi2 = sum |observed - predicted|^2 + 1000 x (images) per unlinked observed image
+ * (src/chi_computation.cpp:11-195).  FP64; the inclusion tests round exactly as the
+ * reference's for the same deflections. */
+#define LT_MAX_IMAGES 20 /* predicted images kept per source (MAXIMPERSOURCE) */
+
+typedef struct {
+    double xmin, xmax, ymin, ymax;     /* the reference's grid_param frame               */
+} lt_frame;
+
+typedef struct {
+    int32_t nsystems;
+    const int32_t *nimages;            /* observed images per system (1..40)             */
+    const double *x, *y;               /* observed positions, concatenated by system     */
+    const double *dlsds;               /* per system: D_LS/D_OS of its source (dr)       */
+} lt_image_systems;
+
+/* chi2 of one model (host results; synchronous).  images_found (may be NULL) gets the
+ * number of predicted images.  LT_ERR_QUEUE_FULL when a source had more than
+ * LT_MAX_IMAGES predicted images (the first LT_MAX_IMAGES were used). */
+lt_status lt_chi2(lt_context *ctx, const lt_catalog *cat, const lt_frame *frame, int32_t n,
+                  const lt_image_systems *systems, double *chi2, int32_t *images_found);
+/* chi2 of `nmodels` models against the same systems (chi2[m], images_found[m]). */
+lt_status lt_chi2_batch(lt_context *ctx, const lt_catalog *const *cats, int32_t nmodels, const lt_frame *frame,
+                        int32_t n, const lt_image_systems *systems, double *chi2, int32_t *images_found);
+/* Write a host map (nx * ny float64, row j at image row j + 1) as a FITS primary image in
+ * the reference's layout (module_writeFits_Image, src/module_writeFits.cpp:113-206):
+ * float32 data, BZERO/BSCALE, a linear arcsec WCS with pixel 1 at (xmin, ymin) and
+ * CDELT = (max - min)/(n - 1), ORIGIN and DATE.  No cfitsio; host only. */
+lt_status lt_write_fits(const char *path, const double *map, int32_t nx, int32_t ny, const lt_frame *frame);
+
+/* Predicted images of given source positions (bx, by, dlsds per source) by delensing the
+ * n x n grid: nfound[s] images at fx/fy[s * LT_MAX_IMAGES + k], in the reference's order.
+ * No counterpart as an entry point in the reference (its step 3 of the chi2). */
+lt_status lt_delense(lt_context *ctx, const lt_catalog *cat, const lt_frame *frame, int32_t n, int32_t nsources,
+                     const double *bx, const double *by, const double *dlsds, int32_t *nfound, double *fx,
+                     double *fy);
+
 /* Wait for the context's work on `stream` and report any status a kernel recorded
  * (e.g. LT_ERR_TIMEOUT from a bounded device-side wait).  Asynchronous (device-pointer)
  * calls report such errors here. */
@@ -280,6 +323,12 @@ uint64_t lt_kernel_launch_count(void);
  * (fp32 = 0) or FP32 (fp32 = 1); 0 on failure.  A measurement utility with no
  * counterpart in the reference: the denominator of the grid kernels' roofline. */
 double lt_measure_fma_peak(int fp32, int device);
+
+/* Evaluate, on `device`, the reciprocal and reciprocal square root that the FP64 pair
+ * loops use for their per-pair denominators (hardware approximation + two Newton-Raphson
+ * steps) on n host inputs: a diagnostic for the tests (0 = LT_OK).  No counterpart in the
+ * reference. */
+int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt);
 
 const char *lt_status_string(lt_status status);
 /* Last error message recorded by the context (never NULL). */

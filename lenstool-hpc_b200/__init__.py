@@ -88,6 +88,17 @@ class _ServerStats(C.Structure):
                 ("device_head", C.c_uint64)]
 
 
+class _Frame(C.Structure):
+    _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double)]
+
+
+class _Systems(C.Structure):
+    _fields_ = [("nsystems", C.c_int32), ("nimages", _ip), ("x", _dp), ("y", _dp), ("dlsds", _dp)]
+
+
+MAX_IMAGES = 20
+
+
 class _Cosmo(C.Structure):
     _fields_ = [("model", C.c_int32), ("omegaM", C.c_double), ("omegaX", C.c_double), ("curvature", C.c_double),
                 ("wX", C.c_double), ("wa", C.c_double), ("H0", C.c_double)]
@@ -102,7 +113,7 @@ EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release",
            "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_autotune", "lt_measure_fma_peak",
            "lt_batch_create", "lt_batch_launch", "lt_batch_size", "lt_batch_destroy", "lt_server_create",
            "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
-           "lt_server_get_stats", "lt_server_destroy")
+           "lt_server_get_stats", "lt_server_destroy", "lt_chi2", "lt_chi2_batch", "lt_delense")
 SUMS = {"deflection": 1, "hessian": 2, "potential": 4, "lens": 6}
 
 
@@ -145,6 +156,10 @@ def load_library(path=None):
     L.lt_server_release.argtypes = [vp, C.c_uint64]
     L.lt_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
     L.lt_server_destroy.argtypes = [vp]
+    L.lt_chi2.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems), _dp, _ip]
+    L.lt_chi2_batch.argtypes = [vp, C.POINTER(vp), C.c_int32, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems), _dp,
+                                _ip]
+    L.lt_delense.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.c_int32, _dp, _dp, _dp, _ip, _dp, _dp]
     L.lt_kernel_launch_count.restype = C.c_uint64
     L.lt_status_string.restype = C.c_char_p
     L.lt_status_string.argtypes = [C.c_int]
@@ -333,6 +348,38 @@ class Context:
 
     def synchronize(self, stream=None):
         self._check(self._lib.lt_synchronize(self.handle, _stream_handle(stream)), "lt_synchronize")
+
+    # ---- strong-lensing chi2 (frame = (xmin, xmax, ymin, ymax) of an n x n grid) ----
+
+    def chi2(self, cats, frame, n, systems):
+        """lt_chi2_batch: chi2 of each catalogue (model) against `systems` (an
+        images.ImageSystems).  Returns (chi2 array, predicted-image counts)."""
+        single = not isinstance(cats, (list, tuple))
+        cl = [self._cat(c) for c in ([cats] if single else cats)]
+        s = systems.contiguous()
+        sy = _Systems(s.nsys, s.nimg.ctypes.data_as(_ip), s.x.ctypes.data_as(_dp), s.y.ctypes.data_as(_dp),
+                      s.dr.ctypes.data_as(_dp))
+        handles = (C.c_void_p * len(cl))(*[c.handle.value if hasattr(c.handle, "value") else c.handle for c in cl])
+        chi = np.empty(len(cl))
+        found = np.empty(len(cl), np.int32)
+        st = self._lib.lt_chi2_batch(self.handle, handles, len(cl), C.byref(_Frame(*frame)), n, C.byref(sy),
+                                     chi.ctypes.data_as(_dp), found.ctypes.data_as(_ip))
+        self._check(st, "lt_chi2_batch")
+        return (chi[0], int(found[0])) if single else (chi, found)
+
+    def delense(self, cat, frame, n, bx, by, dlsds):
+        """lt_delense: predicted images of the sources (bx, by, dlsds): (nfound, fx, fy)."""
+        cat = self._cat(cat)
+        bx, by, dr = (np.ascontiguousarray(np.broadcast_to(a, np.shape(bx)), np.float64) for a in (bx, by, dlsds))
+        k = bx.size
+        nf = np.zeros(k, np.int32)
+        fx = np.zeros((k, MAX_IMAGES))
+        fy = np.zeros((k, MAX_IMAGES))
+        st = self._lib.lt_delense(self.handle, cat.handle, C.byref(_Frame(*frame)), n, k, bx.ctypes.data_as(_dp),
+                                  by.ctypes.data_as(_dp), dr.ctypes.data_as(_dp), nf.ctypes.data_as(_ip),
+                                  fx.ctypes.data_as(_dp), fy.ctypes.data_as(_dp))
+        self._check(st, "lt_delense")
+        return nf, fx, fy
 
     def batch(self, requests, precision="fp32c") -> "Batch":
         """lt_batch_create: `requests` are Request objects with device outputs."""

@@ -284,6 +284,7 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
     ctx->shape[LT_FP32C][OP_HESS] = LT_SHAPE(2, 2);
     ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE(2, 2);
     ctx->shape[LT_FP32C][OP_HESS | OP_POT] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP32C][OP_GRAD] = LT_SHAPE(2, 2);
     cudaSetDevice(device);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);

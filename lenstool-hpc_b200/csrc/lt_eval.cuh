@@ -74,9 +74,19 @@ __device__ __forceinline__ void close_run64(Acc64<OP, P> &acc, int kmap, double 
 
 template <int P>
 struct Acc32 {
-    double hxx[P], hyy[P], hxy[P], psi[P]; /* FP64 terms, sky frame */
+    double hxx[P], hyy[P], hxy[P], psi[P], gx[P], gy[P]; /* FP64 terms, sky frame */
     float ks[P], kc[P], g1s[P], g1c[P], g2s[P], g2c[P], ps[P], pc[P]; /* Kahan sums of FP32 terms */
+    float gxs[P], gxc[P], gys[P], gyc[P];
 };
+
+/* Zero the sums of pixel k. */
+template <int P>
+__device__ __forceinline__ void acc32_zero(Acc32<P> &acc, int k)
+{
+    acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = acc.gx[k] = acc.gy[k] = 0.;
+    acc.ks[k] = acc.kc[k] = acc.g1s[k] = acc.g1c[k] = acc.g2s[k] = acc.g2c[k] = 0.f;
+    acc.ps[k] = acc.pc[k] = acc.gxs[k] = acc.gxc[k] = acc.gys[k] = acc.gyc[k] = 0.f;
+}
 
 template <int OP, int P, int TYPE>
 __device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, const double (&px)[P], double py, int kmap,
@@ -96,6 +106,7 @@ __device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, co
                 acc.hxy[k] = hh.xy;
             }
             if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
+            if (OP & OP_GRAD) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
         }
     }
 }
@@ -123,28 +134,38 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
 #pragma unroll
             for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
         }
-        if (!(OP & OP_HESS)) continue;
+        if (!(OP & (OP_HESS | OP_GRAD))) continue;
         if (__any_sync(0xffffffffu, near)) {
             const lt_rec64 &r64 = recs64[r.idx64];
             const double w = kmap ? r64.w : 1.0;
 #pragma unroll
             for (int k = 0; k < P; k++) {
-                Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
-                hess_pair<TYPE>(r64, px[k], py, w, hh);
-                acc.hxx[k] = hh.xx;
-                acc.hyy[k] = hh.yy;
-                acc.hxy[k] = hh.xy;
+                if (OP & OP_HESS) {
+                    Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
+                    hess_pair<TYPE>(r64, px[k], py, w, hh);
+                    acc.hxx[k] = hh.xx;
+                    acc.hyy[k] = hh.yy;
+                    acc.hxy[k] = hh.xy;
+                }
+                if (OP & OP_GRAD) grad_pair<TYPE>(r64, px[k], py, acc.gx[k], acc.gy[k]);
             }
         } else {
             const float w = kmap ? r.w : 1.0f;
 #pragma unroll
             for (int k = 0; k < P; k++) {
-                KG32 t = hess32<TYPE>(r, u[k], v[k]);
-                const float g1 = t.g1 * r.c2t - t.g2 * r.s2t;
-                const float g2 = t.g1 * r.s2t + t.g2 * r.c2t;
-                kahan_add(acc.ks[k], acc.kc[k], w * t.k);
-                kahan_add(acc.g1s[k], acc.g1c[k], w * g1);
-                kahan_add(acc.g2s[k], acc.g2c[k], w * g2);
+                if (OP & OP_HESS) {
+                    KG32 t = hess32<TYPE>(r, u[k], v[k]);
+                    const float g1 = t.g1 * r.c2t - t.g2 * r.s2t;
+                    const float g2 = t.g1 * r.s2t + t.g2 * r.c2t;
+                    kahan_add(acc.ks[k], acc.kc[k], w * t.k);
+                    kahan_add(acc.g1s[k], acc.g1c[k], w * g1);
+                    kahan_add(acc.g2s[k], acc.g2c[k], w * g2);
+                }
+                if (OP & OP_GRAD) {
+                    const G32 t = grad32<TYPE>(r, u[k], v[k]);
+                    kahan_add(acc.gxs[k], acc.gxc[k], t.x * r.cs - t.y * r.sn);
+                    kahan_add(acc.gys[k], acc.gyc[k], t.y * r.cs + t.x * r.sn);
+                }
             }
         }
     }
@@ -168,6 +189,14 @@ __device__ __forceinline__ void fp32c_total(const Acc32<P> &acc, int k, double D
     psi = add(acc.psi[k], sub((double)acc.ps[k], (double)acc.pc[k]));
     const double omk = sub(1., mul(kap, D)), g1d = mul(g1, D), g2d = mul(g2, D);
     det = sub(sub(mul(omk, omk), mul(g1d, g1d)), mul(g2d, g2d));
+}
+
+/* Pixel total of the FP32C deflection sums. */
+template <int P>
+__device__ __forceinline__ void fp32c_grad_total(const Acc32<P> &acc, int k, double &gx, double &gy)
+{
+    gx = rn::add(acc.gx[k], rn::sub((double)acc.gxs[k], (double)acc.gxc[k]));
+    gy = rn::add(acc.gy[k], rn::sub((double)acc.gys[k], (double)acc.gyc[k]));
 }
 
 } // namespace lt

@@ -240,9 +240,7 @@ __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args
 #pragma unroll
             for (int k = 0; k < P; k++) {
                 px[k] = pixel_x(a, (ix + k) < a.nx ? ix + k : a.nx - 1);
-                acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
-                acc.ks[k] = acc.kc[k] = acc.g1s[k] = acc.g1c[k] = acc.g2s[k] = acc.g2c[k] = 0.f;
-                acc.ps[k] = acc.pc[k] = 0.f;
+                acc32_zero(acc, k);
             }
         }
         if (tid == 0 && s + 1 < steps) issue(s + 1);
@@ -276,12 +274,13 @@ __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args
 
         if (ci == A.nchunks - 1 && iy < a.ny) {
             const long row = (long)iy * a.nx;
-            double hxx[P], hyy[P], hxy[P], psi[P];
+            double hxx[P], hyy[P], hxy[P], psi[P], gx[P], gy[P];
             bool flag[P];
 #pragma unroll
             for (int k = 0; k < P; k++) {
                 double det;
                 fp32c_total(acc, k, a.D, hxx[k], hyy[k], hxy[k], psi[k], det);
+                fp32c_grad_total(acc, k, gx[k], gy[k]);
                 flag[k] = (OP & OP_HESS) && !(fabs(det) * A.mu_flag >= 1.0);
             }
             const bool full = a.vec_ok && (ix + P <= a.nx);
@@ -289,7 +288,7 @@ __global__ void __launch_bounds__(kThreads32, MINB) grid32c_kernel(const C32Args
                 double v[P];
 #pragma unroll
                 for (int k = 0; k < P; k++)
-                    v[k] = map_value(a.kinds[o], 0., 0., hxx[k], hyy[k], hxy[k], psi[k], a.D, a.mult, a.scale);
+                    v[k] = map_value(a.kinds[o], gx[k], gy[k], hxx[k], hyy[k], hxy[k], psi[k], a.D, a.mult, a.scale);
                 double *dst = a.out[o] + row + ix;
                 if (P == 2 && full) {
                     *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1 % P]);
@@ -329,6 +328,7 @@ static void (*pick_kernel32(int op, int shape))(const C32Args)
     case OP_HESS: return pick_shape32<OP_HESS>(shape);
     case OP_POT: return pick_shape32<OP_POT>(shape);
     case OP_HESS | OP_POT: return pick_shape32<OP_HESS | OP_POT>(shape);
+    case OP_GRAD: return pick_shape32<OP_GRAD>(shape);
     default: return nullptr;
     }
 }
@@ -344,8 +344,8 @@ int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, vo
 {
     cudaStream_t s = (cudaStream_t)stream;
     const Fp32cCatalog &fc = *reinterpret_cast<const Fp32cCatalog *>(&cat->aux_desc);
-    if (op & OP_GRAD) {
-        set_error(ctx, "FP32C is implemented for the Hessian maps; use LT_FP64 for deflections");
+    if ((op & OP_GRAD) && op != OP_GRAD) {
+        set_error(ctx, "FP32C deflection grids are computed on their own");
         return (int)cudaErrorNotSupported;
     }
     int err = cudaSuccess;

@@ -66,3 +66,35 @@ extern "C" double lt_measure_fma_peak(int fp32, int device)
 {
     return fp32 ? measure<float>(device) : measure<double>(device);
 }
+
+/* ---- the per-pair reciprocal and reciprocal square root (lt_profiles64.cuh) ---- */
+
+#include "lt_profiles64.cuh"
+
+namespace {
+__global__ void fast_math_kernel(const double *x, double *rcp, double *rsq, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        rcp[i] = lt::rcp64(x[i]);
+        rsq[i] = lt::rsqrt64(x[i]);
+    }
+}
+} // namespace
+
+extern "C" int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt)
+{
+    if (n < 1 || !x || !rcp || !rsqrt) return 1;
+    if (cudaSetDevice(device) != cudaSuccess) return 4;
+    double *d = nullptr;
+    const size_t b = sizeof(double) * (size_t)n;
+    if (cudaMalloc(&d, 3 * b) != cudaSuccess) return 5;
+    cudaError_t e = cudaMemcpy(d, x, b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        fast_math_kernel<<<256, 256>>>(d, d + n, d + 2 * n, n);
+        lt::count_launch(1);
+        e = cudaMemcpy(rcp, d + n, b, cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(rsqrt, d + 2 * n, b, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : 4;
+}

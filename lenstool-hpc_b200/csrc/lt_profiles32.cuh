@@ -126,6 +126,60 @@ __device__ __forceinline__ KG32 hess32(const lt_rec32 &h, float u, float v)
     return r;
 }
 
+struct G32 {
+    float x, y; /* halo-frame deflection */
+};
+
+/* Deflection, FP32.  The reference writes the PIEMD deflection as
+ * pref (arg z, -log|z|) with z = N/D, N = cx1 u + i(2 sqrt(e) w - v/cx1),
+ * D = u + i(2 r sqrt(e) - v), w = sqrt(r^2 + rho^2) (the KERNEL of src/gradient.cpp:
+ * 548-607, 744-811; pref = ci b0 [rcut/(rcut - rc)]), and the cut dPIE as the difference
+ * of the core and cut terms, which cancel far from the halo.  Here that difference is
+ * log(z_c/z_t) = log(1 + eps) with eps = (dN D_t - dD N_t)/(D_c N_t), built from the exact
+ * differences dN = N_c - N_t = i 2 sqrt(e) (w_c - w_t), w_c - w_t = (rc^2 - rcut^2)/(w_c + w_t),
+ * and dD = i 2 sqrt(e) (rc - rcut): no digit is lost to the cancellation, and
+ * Re log(1 + eps) = log1p(2 eps_r + |eps|^2)/2, Im = atan2(eps_i, 1 + eps_r).  (The
+ * reference's two arguments never straddle the branch cut here: arg z_c - arg z_t equals
+ * arg(z_c/z_t), checked over the workload catalogues.)  SIS (src/gradient.cpp:260-299):
+ * b0 ((1-e) u, (1+e) v)/sqrt((1-e) u^2 + (1+e) v^2). */
+template <int TYPE>
+__device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
+{
+    if (TYPE == 5) {
+        const float ir = rsqrtf(u * u * h.cx1 + v * v * h.icx1);
+        return {h.ppre * h.cx1 * u * ir, h.ppre * h.icx1 * v * ir};
+    }
+    const float rho2 = u * u * h.cxi + v * v * h.cyi;
+    const float xc = h.rc2 + rho2;
+    const float wc = xc * rsqrtf(xc);
+    const float nr = h.cx1 * u;
+    const float dci = h.s2rc - v;
+    if (TYPE == 8) {
+        const float nci = h.s2 * wc - v * h.icx1;
+        /* z = N/D: log|z| = (log|N|^2 - log|D|^2)/2, arg z = arg(N conj(D)) */
+        const float lr = 0.5f * (logf(nr * nr + nci * nci) - logf(u * u + dci * dci));
+        const float li = atan2f(nci * u - nr * dci, nr * u + nci * dci);
+        return {h.ppre * li, -h.ppre * lr};
+    }
+    const float xt = h.rcut2 + rho2;
+    const float wt = xt * rsqrtf(xt);
+    const float dw = h.dr2 * frcp(wc + wt);
+    const float nti = h.s2 * wt - v * h.icx1;
+    const float dti = h.s2rcut - v;
+    const float dni = h.s2 * dw, ddi = h.s2 * h.drs;
+    /* num = i dni D_t - i ddi N_t,  den = D_c N_t */
+    const float numr = ddi * nti - dni * dti;
+    const float numi = dni * u - ddi * nr;
+    const float denr = u * nr - dci * nti;
+    const float deni = u * nti + dci * nr;
+    const float inv = frcp(denr * denr + deni * deni);
+    const float er = (numr * denr + numi * deni) * inv;
+    const float ei = (numi * denr - numr * deni) * inv;
+    const float lr = 0.5f * log1pf(er * (2.f + er) + ei * ei);
+    const float li = atan2f(ei, 1.f + er);
+    return {h.ppre * li, -h.ppre * lr};
+}
+
 /* Potential, FP32.  pi05 of src/potential_GPU.cu:47-72 evaluated through identities that
  * remove its transcendental functions except the two complex logarithms per radius:
  *   exp(eta_re) = exp(-asinh(s)/2) = (|s| + sqrt(s^2 + 1))^(-sign(s)/2),  s = e1 v/z,

@@ -137,7 +137,7 @@ __device__ __forceinline__ void tile_pixel(const GridArgs &a, int tile, int &ix,
  * Hessian (OP_HEX) or the fast one (OP_HESS), potential.  Writes the output planes of
  * the deflection kinds when OP is OP_GRAD, the others otherwise. */
 template <int OP, int P>
-__device__ bool tile64(const QItem &it, int tile, Stage &st, int32_t *status)
+__device__ __noinline__ bool tile64(const QItem &it, int tile, Stage &st, int32_t *status)
 {
     const GridArgs &a = it.g;
     int ix, iy;
@@ -201,7 +201,7 @@ __device__ bool tile64(const QItem &it, int tile, Stage &st, int32_t *status)
  * grid32c_kernel's per-tile work followed by the FP64 recomputation of the tile's
  * pixels with |mu| > mu_flag (the single-grid path's second pass, same arithmetic). */
 template <int OP, int P>
-__device__ bool tile32(const QItem &it, int tile, Stage &st, int32_t *status, int16_t *s_list, int *s_count)
+__device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_t *status, int16_t *s_list, int *s_count)
 {
     const GridArgs &a = it.g;
     int ix, iy;
@@ -212,9 +212,7 @@ __device__ bool tile32(const QItem &it, int tile, Stage &st, int32_t *status, in
 #pragma unroll
     for (int k = 0; k < P; k++) {
         px[k] = pixel_x(a, (ix + k) < a.nx ? ix + k : a.nx - 1);
-        acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
-        acc.ks[k] = acc.kc[k] = acc.g1s[k] = acc.g1c[k] = acc.g2s[k] = acc.g2c[k] = 0.f;
-        acc.ps[k] = acc.pc[k] = 0.f;
+        acc32_zero(acc, k);
     }
     bool ok = walk_chunks(st, it.chunks32, it.nchunks32, a.recs, it.recs32, status,
                           [&](const lt_chunk &c, const unsigned char *buf) {
@@ -242,22 +240,23 @@ __device__ bool tile32(const QItem &it, int tile, Stage &st, int32_t *status, in
     if (recompute) __syncthreads();
     if (iy < a.ny) {
         const long row = (long)iy * a.nx;
-        double hxx[P], hyy[P], hxy[P], psi[P];
+        double hxx[P], hyy[P], hxy[P], psi[P], gx[P], gy[P];
         bool flag[P];
 #pragma unroll
         for (int k = 0; k < P; k++) {
             double det;
             fp32c_total(acc, k, a.D, hxx[k], hyy[k], hxy[k], psi[k], det);
+            fp32c_grad_total(acc, k, gx[k], gy[k]);
             flag[k] = recompute && !(fabs(det) * it.mu_flag >= 1.0);
         }
         const bool full = a.vec_ok && (ix + P <= a.nx);
         for (int o = 0; o < a.nout; o++) {
             const int kind = a.kinds[o];
-            if (is_grad_kind(kind)) continue;
+            if (is_grad_kind(kind) != (OP == OP_GRAD)) continue;
             double v[P];
 #pragma unroll
             for (int k = 0; k < P; k++)
-                v[k] = map_value(kind, 0., 0., hxx[k], hyy[k], hxy[k], psi[k], a.D, a.mult, a.scale);
+                v[k] = map_value(kind, gx[k], gy[k], hxx[k], hyy[k], hxy[k], psi[k], a.D, a.mult, a.scale);
             double *dst = a.out[o] + row + ix;
             if (P == 2 && full) {
                 *reinterpret_cast<double2 *>(dst) = make_double2(v[0], v[1 % P]);
@@ -403,16 +402,14 @@ __global__ void __launch_bounds__(kQThreads, 2) queue_kernel(const QArgs q)
         bool ok = true;
         const int hp = item.op & (OP_HESS | OP_POT);
         if (MODE == QMODE_C32) {
-            if (item.op & OP_GRAD) ok = tile64<OP_GRAD, 2>(item, tile, st, q.status);
+            if (item.op & OP_GRAD) ok = tile32<OP_GRAD, 2>(item, tile, st, q.status, s_list, &s_count);
             if (ok && hp == OP_HESS) ok = tile32<OP_HESS, 2>(item, tile, st, q.status, s_list, &s_count);
             if (ok && hp == OP_POT) ok = tile32<OP_POT, 2>(item, tile, st, q.status, s_list, &s_count);
             if (ok && hp == (OP_HESS | OP_POT))
                 ok = tile32<OP_HESS | OP_POT, 2>(item, tile, st, q.status, s_list, &s_count);
-        } else if (item.ppt == 2) {
+        } else if (item.ppt == 2) { /* requests without the potential */
             if (item.op & OP_GRAD) ok = tile64<OP_GRAD, 2>(item, tile, st, q.status);
             if (ok && hp == OP_HESS) ok = tile64<OP_HEX, 2>(item, tile, st, q.status);
-            if (ok && hp == OP_POT) ok = tile64<OP_POT, 2>(item, tile, st, q.status);
-            if (ok && hp == (OP_HESS | OP_POT)) ok = tile64<OP_HEX | OP_POT, 2>(item, tile, st, q.status);
         } else {
             if (item.op & OP_GRAD) ok = tile64<OP_GRAD, 1>(item, tile, st, q.status);
             if (ok && hp == OP_HESS) ok = tile64<OP_HEX, 1>(item, tile, st, q.status);

@@ -19,6 +19,7 @@
  */
 #include <math.h>
 #include <stddef.h>
+#include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -592,4 +593,176 @@ int lto_map(int kind, long np, const double *a, const double *b, const double *c
         out[p] = r;
     }
     return LTO_OK;
+}
+
+/* ---------------------------------------------------------------------------------- */
+/* strong-lensing chi2 by barycentric delensing                                       */
+/* ---------------------------------------------------------------------------------- */
+
+/* At most this many predicted images per source (MAXIMPERSOURCE,
+ * src/structure_hpc.hpp:41); a source with more reports LTO_ERR_ARG. */
+#define LTO_MAXIMG 20
+
+/* Source of each multiple-image system: the mean of its images' source-plane positions
+ * theta - dr alpha(theta), alpha evaluated at each observed image
+ * (src/chi_CPU_barycenter.cpp:180-214). */
+int lto_source_barycenters(const lto_cat *c, int nsys, const int *nimg, const double *ix, const double *iy,
+                           const double *dr, double *bx, double *by)
+{
+    int idx = 0;
+    for (int s = 0; s < nsys; s++) {
+        double sx = 0., sy = 0.;
+        for (int i = 0; i < nimg[s]; i++) {
+            double ax, ay;
+            int st = grad_point(c, ix[idx + i], iy[idx + i], &ax, &ay);
+            if (st) return st;
+            sx += ix[idx + i] - dr[s] * ax;
+            sy += iy[idx + i] - dr[s] * ay;
+        }
+        bx[s] = sx / nimg[s];
+        by[s] = sy / nimg[s];
+        idx += nimg[s];
+    }
+    return LTO_OK;
+}
+
+typedef struct { double x, y; } lto_pt;
+
+/* mychi_determinant, src/delense_CPU_utils.hpp:127-136 */
+static double tri_det(lto_pt A, lto_pt B, lto_pt C)
+{
+    return B.x * C.y - B.y * C.x + A.x * B.y - A.y * B.x + A.y * C.x - A.x * C.y;
+}
+
+/* mychi_inside / mychi_insideborder (identical tests), src/delense_CPU_utils.hpp:146-209 */
+static int tri_inside(lto_pt P, lto_pt a, lto_pt b, lto_pt cc)
+{
+    double d = tri_det(a, b, cc);
+    if (tri_det(a, b, P) * d < 0.) return 0;
+    if (tri_det(b, cc, P) * d < 0.) return 0;
+    if (tri_det(cc, a, P) * d < 0.) return 0;
+    return 1;
+}
+
+/* delense_barycenter, src/delense_CPU.cpp:6-140, in its serial order (rows, then
+ * columns; the upper triangle of a cell is tested first): every grid cell whose upper or
+ * lower triangle, mapped to the source plane with the deflection grid (ax, ay: n x n,
+ * pixel (i, j) at xmin + i dx, ymin + j dy, dx = (xmax - xmin)/(n - 1)), contains a
+ * system's source adds the image-plane triangle's barycentre as a predicted image
+ * (src/delense_CPU_utils.hpp:81-106, 215-225). */
+int lto_delense(int n, double xmin, double xmax, double ymin, double ymax, const double *ax, const double *ay,
+                int nsys, const double *bx, const double *by, const double *dr, int *nfound, double *fx, double *fy)
+{
+    const double dx = (xmax - xmin) / (n - 1), dy = (ymax - ymin) / (n - 1);
+    int overflow = 0;
+    for (int s = 0; s < nsys; s++) {
+        const lto_pt P = {bx[s], by[s]};
+        const double d = dr[s];
+        int k = 0;
+        for (int y = 0; y < n - 1; y++)
+            for (int x = 0; x < n - 1; x++) {
+                const double xp = xmin + x * dx, yp = ymin + y * dy;
+                const long g = (long)y * n + x;
+                /* upper: a = (x, y), b = (x, y + dy), c = (x + dx, y) */
+                lto_pt ia = {xp, yp}, ib = {xp, yp + dy}, ic = {xp + dx, yp};
+                lto_pt sa = {ia.x - d * ax[g], ia.y - d * ay[g]};
+                lto_pt sb = {ib.x - d * ax[g + n], ib.y - d * ay[g + n]};
+                lto_pt sc = {ic.x - d * ax[g + 1], ic.y - d * ay[g + 1]};
+                int found = tri_inside(P, sa, sb, sc);
+                if (!found) {
+                    /* lower: a = (x + dx, y + dy), b = (x + dx, y), c = (x, y + dy) */
+                    ia.x = xp + dx; ia.y = yp + dy;
+                    ib.x = xp + dx; ib.y = yp;
+                    ic.x = xp; ic.y = yp + dy;
+                    sa.x = ia.x - d * ax[g + n + 1]; sa.y = ia.y - d * ay[g + n + 1];
+                    sb.x = ib.x - d * ax[g + 1]; sb.y = ib.y - d * ay[g + 1];
+                    sc.x = ic.x - d * ax[g + n]; sc.y = ic.y - d * ay[g + n];
+                    found = tri_inside(P, sa, sb, sc);
+                }
+                if (found) {
+                    if (k < LTO_MAXIMG) {
+                        fx[s * LTO_MAXIMG + k] = (ia.x + ib.x + ic.x) / 3.;
+                        fy[s * LTO_MAXIMG + k] = (ia.y + ib.y + ic.y) / 3.;
+                    } else {
+                        overflow = 1;
+                    }
+                    k++;
+                }
+            }
+        nfound[s] = k < LTO_MAXIMG ? k : LTO_MAXIMG;
+    }
+    return overflow ? LTO_ERR_ARG : LTO_OK;
+}
+
+static double pt_dist(double ax, double ay, double bx, double by)
+{
+    double x = ax - bx, y = ay - by;
+    return sqrt(x * x + y * y);
+}
+
+/* chi_computation, src/chi_computation.cpp:11-195: each predicted image is linked to its
+ * closest observed image (a second one competing for the same observed image goes to
+ * the closest observed image not yet linked, with the reference's loop bounds), then
+ * chi2 = sum over linked observed images of |observed - predicted|^2 plus 1000 x
+ * (images of the system) for every observed image left without a predicted one.
+ * Returns chi2; *images_found counts the predicted images. */
+double lto_chi2_images(int nsys, const int *nimg, const double *ix, const double *iy, const int *nfound,
+                       const double *fx, const double *fy, int *images_found)
+{
+    double chi = 0.;
+    int index = 0;
+    *images_found = 0;
+    for (int s = 0; s < nsys; s++) {
+        const int n = nimg[s];
+        int linked[LTO_MAXIMG];
+        double tx[LTO_MAXIMG], ty[LTO_MAXIMG], dist[LTO_MAXIMG];
+        memset(linked, 0, sizeof(linked));
+        for (int ii = 0; ii < nfound[s]; ii++) {
+            const double px = fx[s * LTO_MAXIMG + ii], py = fy[s * LTO_MAXIMG + ii];
+            int im = 0;
+            dist[0] = pt_dist(px, py, ix[index], iy[index]);
+            for (int i = 1; i < n; i++) {
+                dist[i] = pt_dist(px, py, ix[index + i], iy[index + i]);
+                if (dist[i] < dist[im]) im = i;
+            }
+            (*images_found)++;
+            if (linked[im] == 0) {
+                tx[im] = px;
+                ty[im] = py;
+                linked[im]++;
+            } else {
+                double tempx, tempy;
+                if (dist[im] < pt_dist(ix[index + im], iy[index + im], tx[im], ty[im])) {
+                    tempx = tx[im];
+                    tempy = ty[im];
+                    tx[im] = px;
+                    ty[im] = py;
+                } else {
+                    tempx = px;
+                    tempy = py;
+                }
+                int second = 0;
+                for (int i = 1; i < n && (i != im); i++)
+                    if (dist[i] > dist[second]) second = i;
+                for (int i = 0; i < n && linked[i] == 0; i++)
+                    if (dist[i] < dist[second]) {
+                        second = i;
+                        im = i;
+                        tx[im] = tempx;
+                        ty[im] = tempy;
+                    }
+                linked[im]++;
+            }
+        }
+        for (int i = 0; i < n; i++) {
+            if (linked[i] > 0) {
+                const double p1 = ix[index + i] - tx[i], p2 = iy[index + i] - ty[i];
+                chi += p1 * p1 + p2 * p2;
+            } else {
+                chi += 1000. * n;
+            }
+        }
+        index += n;
+    }
+    return chi;
 }

@@ -80,6 +80,10 @@ class Oracle:
         L.lto_hess_points.argtypes = [C.POINTER(_Cat), C.c_long, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp, C.c_int]
         L.lto_pot_points.argtypes = [C.POINTER(_Cat), C.c_long, _dp, _dp, _dp, C.c_int]
         L.lto_map.argtypes = [C.c_int, C.c_long, _dp, _dp, _dp, C.c_double, C.c_double, _dp]
+        L.lto_source_barycenters.argtypes = [C.POINTER(_Cat), C.c_int, _ip, _dp, _dp, _dp, _dp, _dp]
+        L.lto_delense.argtypes = [C.c_int] + [C.c_double] * 4 + [_dp, _dp, C.c_int, _dp, _dp, _dp, _ip, _dp, _dp]
+        L.lto_chi2_images.argtypes = [C.c_int, _ip, _dp, _dp, _ip, _dp, _dp, _ip]
+        L.lto_chi2_images.restype = C.c_double
 
     def _cat(self, cat):
         t, fl = _arrays(cat)
@@ -145,6 +149,50 @@ class Oracle:
         return out
 
 
+    # ---- strong-lensing chi2 (systems: nimg int array, ix/iy concatenated images, dr
+    # per system; frame = (xmin, xmax, ymin, ymax) of an n x n grid) ----
+    MAXIMG = 20
+
+    def source_barycenters(self, cat, nimg, ix, iy, dr):
+        s, keep = self._cat(cat)
+        nimg = np.ascontiguousarray(nimg, np.int32)
+        ix, iy, dr = (np.ascontiguousarray(a, np.float64) for a in (ix, iy, dr))
+        bx = np.empty(nimg.size); by = np.empty(nimg.size)
+        self._check(self.lib.lto_source_barycenters(C.byref(s), nimg.size, nimg.ctypes.data_as(_ip), _d(ix), _d(iy),
+                                                    _d(dr), _d(bx), _d(by)))
+        return bx, by
+
+    def delense(self, n, frame, ax, ay, bx, by, dr):
+        """Predicted images (delense_barycenter order): (nfound[nsys], fx, fy[nsys, 20])."""
+        ax, ay, bx, by, dr = (np.ascontiguousarray(a, np.float64).ravel() for a in (ax, ay, bx, by, dr))
+        ns = bx.size
+        nf = np.zeros(ns, np.int32)
+        fx = np.zeros(ns * self.MAXIMG); fy = np.zeros(ns * self.MAXIMG)
+        self._check(self.lib.lto_delense(n, *frame, _d(ax), _d(ay), ns, _d(bx), _d(by), _d(dr),
+                                         nf.ctypes.data_as(_ip), _d(fx), _d(fy)))
+        return nf, fx.reshape(ns, self.MAXIMG), fy.reshape(ns, self.MAXIMG)
+
+    def chi2_images(self, nimg, ix, iy, nfound, fx, fy):
+        nimg = np.ascontiguousarray(nimg, np.int32)
+        nfound = np.ascontiguousarray(nfound, np.int32)
+        ix, iy, fx, fy = (np.ascontiguousarray(a, np.float64).ravel() for a in (ix, iy, fx, fy))
+        found = C.c_int()
+        chi = self.lib.lto_chi2_images(nimg.size, nimg.ctypes.data_as(_ip), _d(ix), _d(iy),
+                                       nfound.ctypes.data_as(_ip), _d(fx), _d(fy), C.byref(found))
+        return chi, found.value
+
+    def chi2(self, cat, frame, n, nimg, ix, iy, dr):
+        """chi2 of one model: deflection grid, source barycentres, delensing, image matching."""
+        from types import SimpleNamespace
+        g = SimpleNamespace(xmin=frame[0], ymin=frame[2], dx=(frame[1] - frame[0]) / (n - 1),
+                            dy=(frame[3] - frame[2]) / (n - 1), nx=n, ny=n, istart=0, jstart=0)
+        ax, ay = self.grad_grid(cat, g)
+        bx, by = self.source_barycenters(cat, nimg, ix, iy, dr)
+        nf, fx, fy = self.delense(n, frame, ax, ay, bx, by, dr)
+        chi, found = self.chi2_images(nimg, ix, iy, nf, fx, fy)
+        return {"chi2": chi, "images_found": found, "nfound": nf, "fx": fx, "fy": fy, "bx": bx, "by": by}
+
+
 class RefLib:
     """The reference's own CPU code (and GPU kernels compiled for the host)."""
 
@@ -161,6 +209,8 @@ class RefLib:
         L.ltref_hess_points.argtypes = soa + [C.c_long, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ltref_pot81_points.argtypes = soa + [C.c_long, _dp, _dp, _dp]
         L.ltref_gpu_kernel_grid.argtypes = [C.c_int] + soa + [C.c_double] * 4 + [C.c_int] * 4 + [_dp] * 4
+        L.ltref_chi2.argtypes = soa + [C.c_double] * 4 + [C.c_int, C.c_int, _ip, _dp, _dp, _dp, _dp, _ip, _ip,
+                                                          _dp, _dp]
 
     @staticmethod
     def _soa(cat):
@@ -220,3 +270,18 @@ class RefLib:
         if which == "pot":
             return out[0].reshape(g.ny, g.nx)
         return tuple(o.reshape(g.ny, g.nx) for o in out)
+
+    def chi2(self, cat, frame, n, nimg, ix, iy, dr):
+        """The reference's chi2 of one model (delense_barycenter + chi_computation)."""
+        s, keep = self._soa(cat)
+        nimg = np.ascontiguousarray(nimg, np.int32)
+        ix, iy, dr = (np.ascontiguousarray(a, np.float64) for a in (ix, iy, dr))
+        ns = nimg.size
+        chi = C.c_double()
+        found = C.c_int()
+        nf = np.zeros(ns, np.int32)
+        fx = np.zeros(ns * 20); fy = np.zeros(ns * 20)
+        self.lib.ltref_chi2(*s, *frame, n, ns, nimg.ctypes.data_as(_ip), _d(ix), _d(iy), _d(dr), C.byref(chi),
+                            C.byref(found), nf.ctypes.data_as(_ip), _d(fx), _d(fy))
+        return {"chi2": chi.value, "images_found": found.value, "nfound": nf, "fx": fx.reshape(ns, 20),
+                "fy": fy.reshape(ns, 20)}

@@ -11,6 +11,8 @@
  *   - gradient2_grid_CPU (src/grid_gradient2_CPU.cpp:54-83) and
  *     module_potentialDerivatives_totalGradient2_SOA (src/gradient2.cpp:226-254);
  *   - amplif_grid_CPU mode 5 (src/grid_amplif_CPU.cpp:38-84);
+ *   - delense_barycenter (src/delense_CPU.cpp:6-140) and chi_computation
+ *     (src/chi_computation.cpp:11-195), the strong-lensing chi2 by barycentric delensing;
  *   - the GPU kernels module_potential_totalPotential_SOA_GPU (src/potential_GPU.cu:139-187),
  *     module_potentialDerivatives_totalGradient2_SOA_GPU (src/gradient2_GPU.cu:337-398) and
  *     module_potentialDerivatives_Kmap_SOA_GPU (src/gradient2_GPU.cu:455-522), compiled as
@@ -20,6 +22,8 @@
 #include <stdlib.h>
 #include <string.h>
 #include <vector>
+
+#include <omp.h>
 
 #include "structure_hpc.hpp"
 
@@ -49,6 +53,12 @@ void module_potentialDerivatives_Kmap_SOA_GPU(type_t *a, type_t *b, type_t *c, t
                                               int nhalos, type_t dx, type_t dy, int nx, int ny, int istart,
                                               int jstart);
 type_t module_potential_81_SOA_GPU(const struct point *p, const struct Potential_SOA *lens, int shalos, int nhalos);
+void delense_barycenter(struct point *image_pos, int *locimagesfound, int *numimg, const runmode_param *runmode,
+                        const struct Potential_SOA *lens, const struct grid_param *frame,
+                        const int *nimages_strongLensing, const struct galaxy *sources, double *grid_gradient_x,
+                        double *grid_gradient_y);
+void chi_computation(double *chi, int *images_found, int *numimagesfound, struct point *imagesposition,
+                     const int *nimages_strongLensing, const galaxy *images, const int nsets);
 
 /* amplif_grid_CPU links against the reference's cosmology module, which needs GSL
  * (absent).  Mode 5 computes dl0s and never uses it; this stand-in returns 0. */
@@ -201,6 +211,94 @@ int ltref_gpu_kernel_grid(int which, SOA_ARGS, double xmin, double ymin, double 
             else
                 module_potentialDerivatives_Kmap_SOA_GPU(o0, o1, o2, o3, &v.soa, &f, n, dx, dy, nx, ny, istart,
                                                          jstart);
+        }
+    }
+    return 0;
+}
+
+/* Strong-lensing chi2 of one model as mychi_bruteforce_SOA_CPU_grid_gradient_barycentersource
+ * computes it (src/chi_CPU_barycenter.cpp:58-287) on one process: the deflection grid
+ * (gradient_grid_CPU over the frame, dx = (xmax - xmin)/(n - 1)), each system's source as
+ * the barycentre of its images mapped with the exact deflection at the image
+ * (:180-214), delense_barycenter on one thread (the reference's serial order; its OpenMP
+ * critical section makes the order of predicted images thread-dependent), the
+ * single-rank part of delense_comm (src/chi_comm.cpp:33-77: a copy), chi_computation.
+ * That driver itself includes mpi.h unconditionally (through chi_comm.hpp) and is not
+ * built here; its steps are repeated in this order. */
+int ltref_chi2(SOA_ARGS, double xmin, double xmax, double ymin, double ymax, int nb, int nsys, const int *nimg,
+               const double *ix, const double *iy, const double *dr, double *chi2, int *images_found, int *nfound,
+               double *fx, double *fy)
+{
+    SoaView v(SOA_PASS);
+    grid_param frame;
+    memset(&frame, 0, sizeof(frame));
+    frame.xmin = xmin;
+    frame.xmax = xmax;
+    frame.ymin = ymin;
+    frame.ymax = ymax;
+    const double dx = (frame.xmax - frame.xmin) / (nb - 1);
+    const double dy = (frame.ymax - frame.ymin) / (nb - 1);
+    std::vector<double> gx((size_t)nb * nb), gy((size_t)nb * nb);
+    gradient_grid_CPU(gx.data(), gy.data(), &frame, &v.soa, n, dx, dy, nb, nb, 0, 0);
+    int total = 0;
+    for (int s = 0; s < nsys; s++) total += nimg[s];
+    std::vector<galaxy> images((size_t)(total > 0 ? total : 1));
+    memset(images.data(), 0, sizeof(galaxy) * images.size());
+    int idx = 0;
+    for (int s = 0; s < nsys; s++)
+        for (int i = 0; i < nimg[s]; i++, idx++) {
+            images[idx].center.x = ix[idx];
+            images[idx].center.y = iy[idx];
+            images[idx].dr = dr[s];
+        }
+    std::vector<galaxy> sources((size_t)nsys);
+    idx = 0;
+    for (int s = 0; s < nsys; s++) {
+        sources[s].center.x = sources[s].center.y = 0.;
+        for (int i = 0; i < nimg[s]; i++) {
+            point Grad = module_potentialDerivatives_totalGradient_SOA(&images[idx + i].center, &v.soa, n);
+            sources[s].center.x += images[idx + i].center.x - images[idx + i].dr * Grad.x;
+            sources[s].center.y += images[idx + i].center.y - images[idx + i].dr * Grad.y;
+        }
+        sources[s].center.x /= nimg[s];
+        sources[s].center.y /= nimg[s];
+        sources[s].dr = images[idx].dr;
+        idx += nimg[s];
+    }
+    runmode_param rm;
+    memset(&rm, 0, sizeof(rm));
+    rm.nsets = nsys;
+    rm.nbgridcells = nb;
+    rm.nhalos = n;
+    std::vector<point> image_pos((size_t)nsys * MAXIMPERSOURCE);
+    memset(image_pos.data(), 0, sizeof(point) * image_pos.size());
+    std::vector<int> loc((size_t)nsys, 0);
+    int numimg = 0;
+    const int threads = omp_get_max_threads();
+    omp_set_num_threads(1);
+    delense_barycenter(image_pos.data(), loc.data(), &numimg, &rm, &v.soa, &frame, nimg, sources.data(), gx.data(),
+                       gy.data());
+    omp_set_num_threads(threads);
+    std::vector<int> numfound((size_t)nsys, 0);
+    std::vector<point> pos((size_t)nsys * MAXIMPERSOURCE);
+    memset(pos.data(), 0, sizeof(point) * pos.size());
+    if (numimg != 0)
+        for (int s = 0; s < nsys; s++) {
+            if (loc[s] == 0) continue;
+            memcpy(&pos[(size_t)s * MAXIMPERSOURCE + numfound[s]], &image_pos[(size_t)s * MAXIMPERSOURCE],
+                   loc[s] * sizeof(point));
+            numfound[s] += loc[s];
+        }
+    double chi = 0.;
+    int found = 0;
+    chi_computation(&chi, &found, numfound.data(), pos.data(), nimg, images.data(), nsys);
+    *chi2 = chi;
+    *images_found = found;
+    for (int s = 0; s < nsys; s++) {
+        nfound[s] = numfound[s];
+        for (int k = 0; k < numfound[s] && k < MAXIMPERSOURCE; k++) {
+            fx[s * MAXIMPERSOURCE + k] = pos[(size_t)s * MAXIMPERSOURCE + k].x;
+            fy[s * MAXIMPERSOURCE + k] = pos[(size_t)s * MAXIMPERSOURCE + k].y;
         }
     }
     return 0;

@@ -51,6 +51,17 @@ def max_rel_err(got, ref, mask=None):
     return float(np.max(np.abs(got - ref) / den))
 
 
+def plane_close(got, exp, kind, precision):
+    """A batch or serving plane against the single-grid call of the same precision.  The
+    Hessian maps must be identical (same pair loops, explicitly rounded epilogues); the
+    deflection and potential planes come from differently inlined code, whose FMA
+    contraction the compiler chooses per kernel: 1e-13 (FP64) or 1e-7 (FP32C) of
+    max(|ref|, RMS)."""
+    if kind in ("potential", "deflection_x", "deflection_y"):
+        return max_rel_err(got, exp) <= (1e-7 if precision == "fp32c" else 1e-13)
+    return np.array_equal(got, exp, equal_nan=True)
+
+
 def golden(name):
     return np.load(GOLDEN / name)
 

@@ -99,3 +99,23 @@ def test_fp32c_host_outputs_and_potential(ctx):
     for k in ("kappa", "gamma1", "gamma2", "mu"):
         assert rel_errors(a[k], b[k], mask) <= TOL32, k
     assert rel_errors(a["psi"], b["psi"], np.ones_like(mask)) <= 1e-6
+
+
+@pytest.mark.parametrize("workload", ["grad_200h_1024", "maps_1000h_4096"])
+def test_fp32c_deflection(ctx, workload):
+    """FP32C deflection (core - cut difference as log(1 + eps) in FP32, cluster-scale
+    halos and near-field pairs in FP64) against LT_FP64, on the workload catalogues over
+    their fields at 768^2."""
+    import torch
+    cat, g0 = catalog.workload(workload)
+    g = catalog.Grid(g0.xmin, g0.xmax, g0.ymin, g0.ymax, 768, 768)
+    res = {}
+    for prec in ("fp32c", "fp64"):
+        ax = torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda")
+        ay = torch.empty_like(ax)
+        ctx.gradient_grid(cat, g, precision=prec, out=(ax, ay))
+        ctx.synchronize()
+        res[prec] = (ax.cpu().numpy(), ay.cpu().numpy())
+    mask = np.ones((g.ny, g.nx), bool)
+    for i in range(2):
+        assert rel_errors(res["fp32c"][i], res["fp64"][i], mask) <= TOL32, (workload, i)

