@@ -129,6 +129,95 @@ lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *soa, lt_catalog 
 lt_status lt_catalog_release(lt_context *ctx, lt_catalog *cat);
 int32_t lt_catalog_nhalos(const lt_catalog *cat);
 
+/* Physical halo parameters of one posterior sample, nhalos entries in the catalogue's
+ * halo order (host arrays, or all device arrays). */
+typedef struct {
+    int32_t nhalos;
+    const double *position_x, *position_y; /* arcsec                                       */
+    const double *vdisp;                   /* km/s; b0 = 6 pi/c^2 vdisp^2 (SIS: 4 pi/c^2)  */
+    const double *ellipticity;             /* mass ellipticity in [0, 1)                   */
+    const double *ellipticity_angle;       /* radians                                      */
+    const double *rcore, *rcut;            /* arcsec                                       */
+    const double *anglecos, *anglesin;     /* optional (NULL: cos/sin of the angle, device) */
+} lt_halo_params;
+
+/* Re-derive a resident catalogue from a new sample on the device, in place and
+ * stream-ordered: b0 and ellipticity_potential as
+ * module_readParameters_calculatePotentialparameter (src/module_readParameters.cpp:
+ * 2808-2871), then the records with the upload's packing arithmetic, so a device update
+ * with the same parameters gives the same records bit for bit.  The types, order, dlsds
+ * and the FP32C chunk lists are kept: a halo of the FP32 class whose new parameters need
+ * FP64 everywhere is evaluated through its FP64 record, an FP64-class halo stays FP64.  A
+ * sample outside a profile's domain makes lt_synchronize report LT_ERR_NONFINITE and
+ * leaves that halo unchanged.  Batches holding the handle see the update on their next
+ * launch; do not update a catalogue that in-flight serving requests use.  Host arrays are
+ * staged in a per-catalogue device buffer: successive updates of one catalogue go on one
+ * stream.  The reference applies a posterior row on the host
+ * (module_readParameters_setbayesmapmodels, src/module_readParameters.cpp:132-227). */
+lt_status lt_catalog_update(lt_context *ctx, lt_catalog *cat, const lt_halo_params *params, void *stream);
+
+/* ---- bayes.dat rows on the device -------------------------------------------------- */
+
+/* The model that bayes.dat rows perturb: the Potential_SOA state of every halo in
+ * catalogue order (host arrays).  Both ellipticities are state, as in
+ * module_readParameters_calculatePotentialparameter_SOA (src/module_readParameters.cpp:
+ * 2873-2936); the state is taken to that step's fixed point before the first row. */
+typedef struct {
+    int32_t nhalos;
+    const int32_t *type;                   /* 5, 8 or 81                                   */
+    const double *position_x, *position_y; /* arcsec                                       */
+    const double *ellipticity_potential;   /* epot                                         */
+    const double *ellipticity;             /* emass                                        */
+    const double *ellipticity_angle;       /* radians                                      */
+    const double *rcore, *vdisp, *rcut;    /* arcsec, km/s, arcsec                         */
+    const double *mag;                     /* magnitudes (potfile galaxies; NULL if none)  */
+} lt_bayes_model;
+
+/* One potfile (setScalingRelations, src/module_readParameters.cpp:1539-1656, ftype 1):
+ * its galaxies are halos first .. first+count-1; a galaxy with mag != 0 gets
+ * rcore = core 10^(0.4 (mag0 - mag)/2), vdisp = sigma 10^(0.4 (mag0 - mag)/vdslope),
+ * rcut = cut 10^(0.4 (mag0 - mag) 2/slope).  Lengths in arcsec. */
+typedef struct {
+    int32_t first, count;
+    double mag0, sigma, cut, core, vdslope, slope;
+} lt_potfile;
+
+/* What one bayes.dat column sets (module_readParameters_setbayesmapmodels,
+ * src/module_readParameters.cpp:142-216). */
+typedef enum {
+    LT_BAYES_SKIP = 0,      /* Nsample, ln(Lhood), image redshifts, Chi2                 */
+    LT_BAYES_X = 1, LT_BAYES_Y = 2, LT_BAYES_EPOT = 3, LT_BAYES_EMASS = 4,
+    LT_BAYES_THETA = 5,     /* degrees                                                    */
+    LT_BAYES_RCORE = 6, LT_BAYES_VDISP = 7, LT_BAYES_RCUT = 8,
+    LT_BAYES_Z = 9,         /* read, no effect on the maps (D_LS/D_OS is set at upload)   */
+    LT_BAYES_POT_CUT = 10,  /* potfile `target`'s cut (arcsec)                            */
+    LT_BAYES_POT_SIGMA = 11 /* potfile `target`'s sigma (km/s)                            */
+} lt_bayes_field;
+
+typedef struct {
+    int32_t field;  /* lt_bayes_field                                     */
+    int32_t target; /* halo index (fields 1-9, not a potfile galaxy) or potfile index */
+} lt_bayes_column;
+
+typedef struct lt_bayes lt_bayes;
+
+/* Upload a model and the meaning of each of a row's ncolumns values. */
+lt_status lt_bayes_create(lt_context *ctx, const lt_bayes_model *model, int32_t npotfiles, const lt_potfile *potfiles,
+                          int32_t ncolumns, const lt_bayes_column *columns, lt_bayes **bayes);
+/* Row r of `rows` (nrows x ncolumns, host or device) applied to the model re-derives
+ * catalogue cats[r] (same halos and types as the model) in place, stream-ordered: one
+ * thread per (row, halo) sets the free parameters, applies the potfile scaling relations
+ * with the row's sigma and cut, takes the potential-parameter step and packs the records
+ * as lt_catalog_update does.  Rows are independent (each starts from the model's state).
+ * With host rows the cos/sin of sampled angles are taken on the host, so the records
+ * equal an upload of the reference's SoA bit for bit; with device rows they are taken on
+ * the device.  Host rows are staged in a per-model device buffer: successive applies of
+ * one model go on one stream.  Replaces the per-sample host update and SoA upload of the
+ * reference's map loop (utils/maps/main.cpp:428-470). */
+lt_status lt_bayes_apply(lt_context *ctx, lt_bayes *bayes, const double *rows, int32_t nrows,
+                         lt_catalog *const *cats, void *stream);
+lt_status lt_bayes_destroy(lt_context *ctx, lt_bayes *bayes);
+
 /* ---- grid evaluators ------------------------------------------------------------- */
 
 /* Deflection grid, both planes multiplied by `scale` (1 for the raw gradient, D_LS/D_OS

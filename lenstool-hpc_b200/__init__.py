@@ -88,6 +88,23 @@ class _ServerStats(C.Structure):
                 ("device_head", C.c_uint64)]
 
 
+class _HaloParams(C.Structure):
+    _fields_ = [("nhalos", C.c_int32)] + [(f, _dp) for f in (
+        "position_x", "position_y", "vdisp", "ellipticity", "ellipticity_angle", "rcore", "rcut", "anglecos",
+        "anglesin")]
+
+
+class _BayesModel(C.Structure):
+    _fields_ = [("nhalos", C.c_int32), ("type", _ip)] + [(f, _dp) for f in (
+        "position_x", "position_y", "ellipticity_potential", "ellipticity", "ellipticity_angle", "rcore", "vdisp",
+        "rcut", "mag")]
+
+
+class _Potfile(C.Structure):
+    _fields_ = [("first", C.c_int32), ("count", C.c_int32)] + [(f, C.c_double) for f in (
+        "mag0", "sigma", "cut", "core", "vdslope", "slope")]
+
+
 class _Frame(C.Structure):
     _fields_ = [("xmin", C.c_double), ("xmax", C.c_double), ("ymin", C.c_double), ("ymax", C.c_double)]
 
@@ -113,7 +130,9 @@ EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release",
            "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_autotune", "lt_measure_fma_peak",
            "lt_batch_create", "lt_batch_launch", "lt_batch_size", "lt_batch_destroy", "lt_server_create",
            "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
-           "lt_server_get_stats", "lt_server_destroy", "lt_chi2", "lt_chi2_batch", "lt_delense")
+           "lt_server_get_stats", "lt_server_destroy", "lt_chi2", "lt_chi2_batch", "lt_delense",
+           "lt_catalog_update", "lt_write_fits", "lt_eval_fast_math", "lt_bayes_create", "lt_bayes_apply",
+           "lt_bayes_destroy")
 SUMS = {"deflection": 1, "hessian": 2, "potential": 4, "lens": 6}
 
 
@@ -156,6 +175,11 @@ def load_library(path=None):
     L.lt_server_release.argtypes = [vp, C.c_uint64]
     L.lt_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
     L.lt_server_destroy.argtypes = [vp]
+    L.lt_catalog_update.argtypes = [vp, vp, C.POINTER(_HaloParams), vp]
+    L.lt_bayes_create.argtypes = [vp, C.POINTER(_BayesModel), C.c_int32, C.POINTER(_Potfile), C.c_int32, _ip,
+                                  C.POINTER(vp)]
+    L.lt_bayes_apply.argtypes = [vp, vp, _dp, C.c_int32, C.POINTER(vp), vp]
+    L.lt_bayes_destroy.argtypes = [vp, vp]
     L.lt_chi2.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems), _dp, _ip]
     L.lt_chi2_batch.argtypes = [vp, C.POINTER(vp), C.c_int32, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems), _dp,
                                 _ip]
@@ -221,6 +245,31 @@ class Catalog:
         if self.handle:
             self.ctx._lib.lt_catalog_release(self.ctx.handle, self.handle)
             self.handle = None
+
+    def update(self, position_x, position_y, vdisp, ellipticity, ellipticity_angle, rcore, rcut, anglecos=None,
+               anglesin=None, stream=None):
+        """lt_catalog_update: re-derive this resident catalogue from a new sample's physical
+        parameters (catalogue halo order; numpy arrays or all torch CUDA tensors)."""
+        arrs = [position_x, position_y, vdisp, ellipticity, ellipticity_angle, rcore, rcut]
+        trig = [anglecos, anglesin] if anglecos is not None and anglesin is not None else [None, None]
+        for a in arrs + trig:
+            if a is not None and (a.shape[0] if hasattr(a, "shape") else len(a)) != self.nhalos:
+                raise LensError(1, f"lt_catalog_update: {self.nhalos} halos expected")
+        keep, ptrs = [], []
+        for a in arrs + trig:
+            if a is None:
+                ptrs.append(None)
+            elif hasattr(a, "data_ptr"):
+                keep.append(a)
+                ptrs.append(C.cast(C.c_void_p(a.data_ptr()), _dp))
+            else:
+                a = np.ascontiguousarray(a, np.float64)
+                keep.append(a)
+                ptrs.append(a.ctypes.data_as(_dp))
+        p = _HaloParams(self.nhalos, *ptrs)
+        st = self.ctx._lib.lt_catalog_update(self.ctx.handle, self.handle, C.byref(p), _stream_handle(stream))
+        self.ctx._check(st, "lt_catalog_update")
+        self._keep = keep
 
     def __del__(self):
         try:
@@ -393,6 +442,62 @@ class Context:
     def server(self, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0) -> "Server":
         """lt_server_create: a continuous-batching serving loop on this context."""
         return Server(self, precision, slots, window, idle_us, output_bytes)
+
+    def bayes(self, model, columns, potfiles=()) -> "Bayes":
+        """lt_bayes_create: a bayes.dat model (bayes.BayesModel), its potfiles
+        (bayes.Potfile) and the meaning of each row column ((field, target) pairs)."""
+        return Bayes(self, model, columns, potfiles)
+
+
+class Bayes:
+    """lt_bayes: bayes.dat rows applied to resident catalogues on the device."""
+
+    def __init__(self, ctx: Context, model, columns, potfiles=()):
+        self.ctx, self.handle = ctx, None
+        arrs = model.arrays()
+        self._keep = [a for a in arrs if a is not None]
+        t, *planes, mag = arrs
+        m = _BayesModel(model.n, t.ctypes.data_as(_ip), *[a.ctypes.data_as(_dp) for a in planes],
+                        None if mag is None else mag.ctypes.data_as(_dp))
+        pots = list(potfiles)
+        parr = (_Potfile * max(1, len(pots)))(*[_Potfile(p.first, p.count, p.mag0, p.sigma, p.cut, p.core, p.vdslope,
+                                                         p.slope) for p in pots])
+        cols = np.ascontiguousarray(np.asarray(columns, np.int32).reshape(-1, 2))
+        self.ncolumns, self.nhalos = cols.shape[0], model.n
+        h = C.c_void_p()
+        st = ctx._lib.lt_bayes_create(ctx.handle, C.byref(m), len(pots), parr, cols.shape[0],
+                                      cols.ctypes.data_as(_ip), C.byref(h))
+        ctx._check(st, "lt_bayes_create")
+        self.handle = h
+
+    def apply(self, rows, cats, stream=None):
+        """Row r of `rows` (numpy nrows x ncolumns, or a torch CUDA tensor) re-derives cats[r]."""
+        cats = list(cats)
+        if hasattr(rows, "data_ptr"):
+            if tuple(rows.shape) != (len(cats), self.ncolumns) or not rows.is_contiguous():
+                raise LensError(1, "lt_bayes_apply: rows must be contiguous (len(cats), ncolumns)")
+            keep, ptr = rows, C.cast(C.c_void_p(rows.data_ptr()), _dp)
+        else:
+            keep = np.ascontiguousarray(rows, np.float64).reshape(-1, self.ncolumns)
+            if keep.shape[0] != len(cats):
+                raise LensError(1, "lt_bayes_apply: one row per catalogue")
+            ptr = keep.ctypes.data_as(_dp)
+        handles = (C.c_void_p * max(1, len(cats)))(*[c.handle for c in cats])
+        st = self.ctx._lib.lt_bayes_apply(self.ctx.handle, self.handle, ptr, len(cats), handles,
+                                          _stream_handle(stream))
+        self.ctx._check(st, "lt_bayes_apply")
+        self._rows = keep
+
+    def destroy(self):
+        if self.handle:
+            self.ctx._lib.lt_bayes_destroy(self.ctx.handle, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
 
 
 class Request:

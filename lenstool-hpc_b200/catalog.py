@@ -151,6 +151,71 @@ def perturb_catalog(base: HaloCatalog, rng: np.random.Generator, rel: float = 0.
 
 
 @dataclasses.dataclass
+class HaloParameters:
+    """The physical parameters a posterior sample varies, in catalogue (type-sorted) order:
+    the inputs of lt_catalog_update (Catalog.update)."""
+    type: np.ndarray
+    position_x: np.ndarray
+    position_y: np.ndarray
+    vdisp: np.ndarray
+    ellipticity: np.ndarray
+    ellipticity_angle: np.ndarray
+    rcore: np.ndarray
+    rcut: np.ndarray
+
+    def catalog(self, z: float = 0.35) -> HaloCatalog:
+        if np.any(np.diff(self.type) < 0):
+            raise ValueError("parameters must be sorted by profile type")
+        return make_catalog(self.type, self.position_x, self.position_y, self.vdisp, self.ellipticity,
+                            self.ellipticity_angle, self.rcore, self.rcut, z=z)
+
+    def perturbed(self, rng: np.random.Generator, rel: float = 0.05) -> "HaloParameters":
+        """p -> p (1 + rel N(0,1)) for vdisp, ellipticity (clipped to [0, 0.95]), angle,
+        rcore and rcut (kept >= 1.5 rcore); positions move by rel (|x| + 1") N(0,1)."""
+        n = self.type.shape[0]
+
+        def jitter(a):
+            return a * (1. + rel * rng.standard_normal(n))
+        x = self.position_x + rel * (np.abs(self.position_x) + 1.) * rng.standard_normal(n)
+        y = self.position_y + rel * (np.abs(self.position_y) + 1.) * rng.standard_normal(n)
+        sig = np.abs(jitter(self.vdisp))
+        e = np.clip(jitter(self.ellipticity), 0., 0.95)
+        th = jitter(self.ellipticity_angle)
+        rc = np.abs(jitter(self.rcore))
+        rcut = np.maximum(np.abs(jitter(self.rcut)), 1.5 * rc)
+        return HaloParameters(self.type.copy(), x, y, sig, e, th, rc, rcut)
+
+    def update_args(self):
+        """The arguments of Catalog.update, with the host's cos/sin of the angle."""
+        return (self.position_x, self.position_y, self.vdisp, self.ellipticity, self.ellipticity_angle, self.rcore,
+                self.rcut, np.cos(self.ellipticity_angle), np.sin(self.ellipticity_angle))
+
+
+def cluster_galaxy_parameters(n_cluster: int, n_galaxy: int, seed: int, cluster_type: int = DPIE) -> HaloParameters:
+    """The physical parameters behind cluster_galaxy_catalog (same draws, same order)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nc, ng = n_cluster, n_galaxy
+    c_sig = rng.uniform(800., 1200., nc)
+    c_rc = rng.uniform(5., 15., nc)
+    c_rcut = np.full(nc, 800.)
+    c_e = rng.uniform(0., 0.6, nc)
+    c_th = rng.uniform(0., math.pi, nc)
+    c_x = rng.uniform(-20., 20., nc)
+    c_y = rng.uniform(-20., 20., nc)
+    g_sig = np.exp(rng.uniform(math.log(80.), math.log(300.), ng))
+    g_rc = rng.uniform(0.05, 0.2, ng)
+    g_rcut = rng.uniform(5., 50., ng)
+    g_e = rng.uniform(0., 0.5, ng)
+    g_th = rng.uniform(0., math.pi, ng)
+    g_x = rng.uniform(-90., 90., ng)
+    g_y = rng.uniform(-90., 90., ng)
+    ptype = np.concatenate([np.full(nc, cluster_type), np.full(ng, DPIE)]).astype(np.int32)
+    cat = lambda a, b: np.concatenate([a, b])  # noqa: E731
+    return HaloParameters(ptype, cat(c_x, g_x), cat(c_y, g_y), cat(c_sig, g_sig), cat(c_e, g_e), cat(c_th, g_th),
+                          cat(c_rc, g_rc), cat(c_rcut, g_rcut))
+
+
+@dataclasses.dataclass
 class Grid:
     """A pixel grid with both endpoints included: x_i = xmin + (i + istart) dx with
     dx = (xmax - xmin)/(n - 1) (src/grid_gradient_CPU.cpp:33-63), stored row-major at

@@ -18,6 +18,7 @@
 #include "lt_grid.cuh"
 #include "lt_halo.h"
 #include "lt_internal.h"
+#include "lt_pack.h"
 
 using namespace lt;
 
@@ -111,49 +112,11 @@ bool lt::is_device_pointer(const void *p)
 
 /* ---------------------------------------------------------------- packing ---- */
 
-/* Per-halo invariants (see lt_halo.h for the slot meaning).  The expressions are the
- * reference's own sub-expressions: src/gradient.cpp:764-783 (cut dPIE deflection),
- * src/gradient2.cpp:57-66 (mdci05), src/potential_GPU.cu:52-58 (pi05). */
+/* Per-halo invariants (lt_halo.h, packed by lt_pack.h). */
 static void pack_one(const lt_halo_soa *s, int i, lt_rec64 &r)
 {
-    const int t = s->type[i];
-    const double e = s->ellipticity_potential[i];
-    const double rc = s->rcore[i], rcut = s->rcut[i], b0 = s->b0[i];
-    memset(&r, 0, sizeof(r));
-    r.x0 = s->position_x[i];
-    r.y0 = s->position_y[i];
-    r.cs = s->anglecos[i];
-    r.sn = s->anglesin[i];
-    r.b0 = b0;
-    r.eps = e;
-    r.rc = rc;
-    r.rcut = rcut;
-    r.w = s->dlsds ? s->dlsds[i] : 1.0;
-    if (t == 5) {
-        r.cx1 = 1. - e;
-        r.cx1inv = 1. + e;
-        r.pref_g = (1. - e) * b0;
-        r.pref_h = (1. + e) * b0;
-        r.ci = b0 * (1. - e) * (1. + e);
-        return;
-    }
-    const double sqe = sqrt(e);
-    r.sqe2 = 2. * sqe;
-    r.cx1 = (1. - e) / (1. + e);
-    r.cx1inv = 1. / r.cx1;
-    r.cxro_inv = 1. / ((1. + e) * (1. + e));
-    r.cyro_inv = 1. / ((1. - e) * (1. - e));
-    r.k4 = 4. * e;
-    r.ci = 0.5 * (1. - e * e) / sqe;
-    const double t05 = (t == 81) ? rcut / (rcut - rc) : 1.0;
-    r.pref_g = r.ci * b0 * t05;
-    r.pref_h = r.ci * b0 * t05;
-    r.rc2 = rc * rc;
-    r.rcut2 = rcut * rcut;
-    r.tsr_c = 2. * rc * sqe;
-    r.tsr_t = 2. * rcut * sqe;
-    r.e1 = 2. * sqe / (1 - e);
-    r.e2 = 2. * sqe / (1 + e);
+    pk::pack64(s->type[i], s->position_x[i], s->position_y[i], s->anglecos[i], s->anglesin[i], s->b0[i],
+               s->ellipticity_potential[i], s->rcore[i], s->rcut[i], s->dlsds ? s->dlsds[i] : 1.0, r);
 }
 
 /* Domain checks: the reference would divide by zero or take sqrt of a negative value
@@ -222,6 +185,7 @@ void lt::free_catalog(lt_context *ctx, lt_catalog *cat)
     dev_free(ctx, cat->recs, sizeof(lt_rec64) * (size_t)cat->nhalos);
     dev_free(ctx, cat->chunks, sizeof(lt_chunk) * (size_t)(cat->nchunks + cat->nchunks_k));
     dev_free(ctx, cat->aux, cat->aux_bytes);
+    dev_free(ctx, cat->stage, cat->stage_bytes);
     delete cat;
 }
 

@@ -131,8 +131,14 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
             near |= (rr < r.rnear2) | (u[k] * u[k] + dv * dv < r.sing_r2) | (rr < r.core_r2);
         }
         if (OP & OP_POT) {
+            if (r.rnear2 == kProxy64) { /* an FP64 proxy record: every term in FP64 */
+                const lt_rec64 &r64 = recs64[r.idx64];
 #pragma unroll
-            for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
+                for (int k = 0; k < P; k++) pot_pair<TYPE>(r64, px[k], py, acc.psi[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
+            }
         }
         if (!(OP & (OP_HESS | OP_GRAD))) continue;
         if (__any_sync(0xffffffffu, near)) {

@@ -25,81 +25,11 @@
 #include "lt_bulk.cuh"
 #include "lt_internal.h"
 #include "lt_eval.cuh"
+#include "lt_pack.h"
 
 namespace lt {
 
-static const double kTau = 0.1;        /* FP64 where b0 / (2 r) > kTau                */
-/* FP64 within (kSingFrac + kSingEps e) rcut of the singular point: the FP32 forms lose
- * accuracy near it, more so at larger ellipticity */
-static const double kSingFrac = 0.3;
-static const double kSingEps = 1.5;
-static const double kCoreFrac = 3.0;   /* FP64 within 3 rcore of the centre           */
 static const double kMuFlag = LT_FP32C_MU_FLAG; /* recompute pixels with |mu| above this (error ~ mu^2) */
-
-static bool needs_fp64_always(const lt_rec64 &r, int type)
-{
-    if (r.b0 >= 5.0) return true;      /* cluster-scale halo */
-    if (type != 5 && r.rc >= 1.0) return true;
-    if (type != 5 && r.eps < 1e-3) return true; /* ci ~ 1/(2 sqrt(e)) amplification */
-    return false;
-}
-
-static void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
-{
-    memset(&o, 0, sizeof(o));
-    o.x0 = r.x0;
-    o.y0 = r.y0;
-    o.cs = (float)r.cs;
-    o.sn = (float)r.sn;
-    o.c2t = (float)(r.cs * r.cs - r.sn * r.sn);
-    o.s2t = (float)(2. * r.cs * r.sn);
-    o.w = (float)r.w;
-    o.type = type;
-    o.idx64 = idx64;
-    const double e = r.eps;
-    const double near_r = r.b0 / (2. * kTau);
-    o.rnear2 = (float)(near_r * near_r);
-    if (type == 5) {
-        o.cx1 = (float)(1. - e);
-        o.icx1 = (float)(1. + e);
-        o.kpre = (float)(r.b0 * (1. - e) * (1. + e));
-        o.ppre = (float)r.b0;
-        o.singv = 0.f;
-        o.sing_r2 = 0.f;
-        o.core_r2 = 0.f;
-        return;
-    }
-    const double sqe = sqrt(e);
-    const double cx1 = (1. - e) / (1. + e);
-    const double ci = 0.5 * (1. - e * e) / sqe;
-    const double t05 = (type == 81) ? r.rcut / (r.rcut - r.rc) : 1.0;
-    o.s2 = (float)(2. * sqe);
-    o.cx1 = (float)cx1;
-    o.icx1 = (float)(1. / cx1);
-    o.cxi = (float)(1. / ((1. + e) * (1. + e)));
-    o.cyi = (float)(1. / ((1. - e) * (1. - e)));
-    o.ome2 = (float)(1. / (1. - e * e));
-    o.e4 = (float)(4. * e);
-    o.cpi = (float)(cx1 + 1. / cx1);
-    o.rc = (float)r.rc;
-    o.rcut = (float)r.rcut;
-    o.drs = (float)(r.rc - r.rcut);
-    o.dr2 = (float)((r.rc - r.rcut) * (r.rc + r.rcut));
-    o.rc2 = (float)(r.rc * r.rc);
-    o.rcut2 = (float)(r.rcut * r.rcut);
-    o.s2rc = (float)(2. * sqe * r.rc);
-    o.s2rcut = (float)(2. * sqe * r.rcut);
-    o.gpre = (float)(0.5 * ci * r.b0 * t05);
-    o.kpre = (float)(type == 81 ? -0.5 * r.b0 * t05 : 0.5 * r.b0);
-    o.ppre = (float)(ci * r.b0 * t05);
-    o.e1 = (float)(2. * sqe / (1. - e));
-    o.e2 = (float)(2. * sqe / (1. + e));
-    const double sr = type == 81 ? r.rcut : r.rc;
-    o.singv = (float)(2. * sr * sqe);
-    const double srad = (kSingFrac + kSingEps * e) * sr;
-    o.sing_r2 = (float)(srad * srad);
-    o.core_r2 = (float)((kCoreFrac * r.rc) * (kCoreFrac * r.rc));
-}
 
 lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
 {
@@ -110,14 +40,15 @@ lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
      * never mix precision or type. */
     std::vector<lt_rec32> r32;
     std::vector<int32_t> t32;
-    std::vector<int32_t> idx64_always, t64;
+    std::vector<int32_t> idx64_always, t64, idx32((size_t)n, -1);
     for (int i = 0; i < n; i++) {
-        if (needs_fp64_always(cat->host_recs[i], types[i])) {
+        if (pk::needs_fp64_always(cat->host_recs[i], types[i])) {
             idx64_always.push_back(i);
             t64.push_back(types[i]);
         } else {
             lt_rec32 o;
-            pack32(cat->host_recs[i], types[i], i, o);
+            pk::pack32(cat->host_recs[i], types[i], i, o);
+            idx32[i] = (int32_t)r32.size();
             r32.push_back(o);
             t32.push_back(types[i]);
         }
@@ -145,16 +76,21 @@ lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
     h.n32 = (int32_t)r32.size();
     h.nchunks = (int32_t)host_chunks.size();
     size_t rb = sizeof(lt_rec32) * r32.size(), cb = sizeof(lt_chunk) * host_chunks.size();
-    size_t total = sizeof(Fp32cCatalog) + rb + cb + 64;
+    const size_t ib = sizeof(int32_t) * (size_t)n;
+    size_t total = sizeof(Fp32cCatalog) + rb + cb + 2 * ib + 64;
     void *mem = nullptr;
     lt_status st = dev_alloc(ctx, &mem, total);
     if (st != LT_OK) return st;
     char *base = (char *)mem;
     h.recs32 = (lt_rec32 *)(base + 64);
     h.chunks = (lt_chunk *)(base + 64 + rb);
+    h.idx32 = (int32_t *)(base + 64 + rb + cb);
+    h.types = h.idx32 + n;
     cudaError_t e = cudaSuccess;
     if (rb) e = cudaMemcpy(h.recs32, r32.data(), rb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && cb) e = cudaMemcpy(h.chunks, host_chunks.data(), cb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && ib) e = cudaMemcpy(h.idx32, idx32.data(), ib, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && ib) e = cudaMemcpy(h.types, types.data(), ib, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         dev_free(ctx, mem, total);
         return cuda_fail(ctx, e, "FP32 catalogue upload");

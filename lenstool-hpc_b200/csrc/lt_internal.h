@@ -38,6 +38,8 @@ struct lt_catalog {
     std::vector<int32_t> host_types;     /* profile type per halo */
     void *aux = nullptr;                 /* FP32C records and chunks, device */
     size_t aux_bytes = 0;
+    void *stage = nullptr;               /* device staging of host parameters (lt_catalog_update) */
+    size_t stage_bytes = 0;
     alignas(16) unsigned char aux_desc[64]; /* FP32C descriptor (host) */
 };
 
@@ -56,6 +58,8 @@ struct Fp32cCatalog {
     lt_chunk *chunks;
     int32_t nchunks;
     int32_t n32;
+    int32_t *idx32;  /* per halo: its FP32 record, or -1 for an FP64-class halo (device) */
+    int32_t *types;  /* per halo profile type (device) */
 };
 
 void count_launch(uint64_t n);

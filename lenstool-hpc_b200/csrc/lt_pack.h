@@ -1,0 +1,208 @@
+/*
+ * lt_pack.h -- per-halo records (lt_rec64, lt_rec32) from the halo parameters, shared by
+ * the host upload (lt_catalog_upload) and the device re-pack (lt_catalog_update).
+ *
+ * Every operation goes through the pk:: helpers: plain IEEE operations on the host (the
+ * host translation units are compiled without FMA contraction) and explicitly rounded
+ * intrinsics on the device, so a record packed on the device equals the host's bit for
+ * bit for the same parameters.
+ *
+ * The expressions are the reference's own per-halo sub-expressions
+ * (src/gradient.cpp:764-783, src/gradient2.cpp:57-66, src/potential_GPU.cu:52-58) and the
+ * potential parameters of module_readParameters_calculatePotentialparameter
+ * (src/module_readParameters.cpp:2808-2871); the FP32 records carry the invariants of the
+ * FP32 forms (lt_profiles32.cuh) and the FP64-fallback radii.
+ */
+#pragma once
+#include <math.h>
+#include <string.h>
+
+#include "lt_halo.h"
+#include "lt_profiles32.cuh"
+
+namespace lt {
+namespace pk {
+
+#if defined(__CUDA_ARCH__)
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double sqr(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ float f32(double a) { return __double2float_rn(a); }
+#else
+inline double mul(double a, double b) { return a * b; }
+inline double add(double a, double b) { return a + b; }
+inline double sub(double a, double b) { return a - b; }
+inline double div(double a, double b) { return a / b; }
+inline double sqr(double a) { return sqrt(a); }
+inline float f32(double a) { return (float)a; }
+#endif
+
+/* FP64 (halo-wide) thresholds of the FP32C path */
+constexpr double kTau = 0.1;       /* FP64 where b0 / (2 r) > kTau                        */
+constexpr double kSingFrac = 0.3;  /* FP64 within (kSingFrac + kSingEps e) r of the       */
+constexpr double kSingEps = 1.5;   /*   singular point of radius r                        */
+constexpr double kCoreFrac = 3.0;  /* FP64 within 3 rcore of the centre                   */
+
+/* b0 and ellipticity_potential from the velocity dispersion and the mass ellipticity
+ * (src/module_readParameters.cpp:2808-2871; pi_c2 = pi / c^2 in arcsec (km/s)^-2). */
+LT_HD inline void potential_parameters(int type, double vdisp, double emass, double &b0, double &eps)
+{
+    const double pi_c2 = 7.209970e-06;
+    if (type == 5) {
+        b0 = mul(mul(mul(4., pi_c2), vdisp), vdisp);
+        eps = div(emass, 3.);
+    } else {
+        b0 = mul(mul(mul(6., pi_c2), vdisp), vdisp);
+        eps = emass == 0. ? 0.00001 : div(sub(1., sqr(sub(1., mul(emass, emass)))), emass);
+    }
+}
+
+/* The FP64 record (slot meaning in lt_halo.h). */
+LT_HD inline void pack64(int t, double x, double y, double cs, double sn, double b0, double e, double rc,
+                         double rcut, double w, lt_rec64 &r)
+{
+    memset(&r, 0, sizeof(r));
+    r.x0 = x;
+    r.y0 = y;
+    r.cs = cs;
+    r.sn = sn;
+    r.b0 = b0;
+    r.eps = e;
+    r.rc = rc;
+    r.rcut = rcut;
+    r.w = w;
+    if (t == 5) {
+        r.cx1 = sub(1., e);
+        r.cx1inv = add(1., e);
+        r.pref_g = mul(sub(1., e), b0);
+        r.pref_h = mul(add(1., e), b0);
+        r.ci = mul(mul(b0, sub(1., e)), add(1., e));
+        return;
+    }
+    const double sqe = sqr(e);
+    r.sqe2 = mul(2., sqe);
+    r.cx1 = div(sub(1., e), add(1., e));
+    r.cx1inv = div(1., r.cx1);
+    r.cxro_inv = div(1., mul(add(1., e), add(1., e)));
+    r.cyro_inv = div(1., mul(sub(1., e), sub(1., e)));
+    r.k4 = mul(4., e);
+    r.ci = div(mul(0.5, sub(1., mul(e, e))), sqe);
+    const double t05 = (t == 81) ? div(rcut, sub(rcut, rc)) : 1.0;
+    r.pref_g = mul(mul(r.ci, b0), t05);
+    r.pref_h = mul(mul(r.ci, b0), t05);
+    r.rc2 = mul(rc, rc);
+    r.rcut2 = mul(rcut, rcut);
+    r.tsr_c = mul(mul(2., rc), sqe);
+    r.tsr_t = mul(mul(2., rcut), sqe);
+    r.e1 = div(mul(2., sqe), sub(1, e));
+    r.e2 = div(mul(2., sqe), add(1, e));
+}
+
+/* module_readParameters_calculatePotentialparameter_SOA (src/module_readParameters.cpp:
+ * 2873-2936) with both ellipticities as state, its branches kept: for SIS the potential
+ * ellipticity drives (emass = 3 epot; emass == 0 with epot != 0 sets epot to 0), for
+ * PIEMD/dPIE the mass ellipticity does (epot = (1 - sqrt(1 - e^2))/e), except emass == 0,
+ * where a non-zero epot sets emass = 2 epot/(1 + epot^2) and a zero one becomes 1e-5. */
+LT_HD inline void calc_potential_parameter(int type, double vdisp, double &emass, double &epot, double &b0)
+{
+    const double pi_c2 = 7.209970e-06;
+    if (type == 5) {
+        b0 = mul(mul(mul(4., pi_c2), vdisp), vdisp);
+        if (emass == 0. && epot != 0.)
+            epot = div(emass, 3.);
+        else
+            emass = mul(epot, 3.);
+    } else {
+        b0 = mul(mul(mul(6., pi_c2), vdisp), vdisp);
+        if (emass == 0. && epot != 0.)
+            emass = div(mul(2., epot), add(1., mul(epot, epot)));
+        else if (emass == 0. && epot == 0.)
+            epot = 0.00001;
+        else
+            epot = div(sub(1., sqr(sub(1., mul(emass, emass)))), emass);
+    }
+}
+
+/* The domain lt_catalog_upload accepts: finite parameters, ellipticity_potential in
+ * [0, 1) (SIS) or (0, 1), rcore > 0 (PIEMD, dPIE), rcut > rcore (dPIE). */
+LT_HD inline bool record_ok(int t, double x, double y, double b0, double cs, double sn, double eps, double rc,
+                            double rcut)
+{
+    if (!isfinite(x) || !isfinite(y) || !isfinite(b0) || !isfinite(cs) || !isfinite(sn) || !isfinite(eps) ||
+        !isfinite(rc) || !isfinite(rcut))
+        return false;
+    if (t == 5 ? !(eps >= 0. && eps < 1.) : !(eps > 0. && eps < 1.)) return false;
+    if (t != 5 && !(rc > 0.)) return false;
+    if (t == 81 && !(rcut > rc)) return false;
+    return true;
+}
+
+/* Halos summed in FP64 for every pixel by the FP32C path: cluster-scale (b0 >= 5"),
+ * large cores (rcore >= 1"), nearly circular PIEMD/dPIE (ci ~ 1/(2 sqrt(e))). */
+LT_HD inline bool needs_fp64_always(const lt_rec64 &r, int type)
+{
+    if (r.b0 >= 5.0) return true;
+    if (type != 5 && r.rc >= 1.0) return true;
+    if (type != 5 && r.eps < 1e-3) return true;
+    return false;
+}
+
+/* The FP32 record of an FP32-class halo (the invariants of lt_profiles32.cuh). */
+LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
+{
+    memset(&o, 0, sizeof(o));
+    o.x0 = r.x0;
+    o.y0 = r.y0;
+    o.cs = f32(r.cs);
+    o.sn = f32(r.sn);
+    o.c2t = f32(sub(mul(r.cs, r.cs), mul(r.sn, r.sn)));
+    o.s2t = f32(mul(mul(2., r.cs), r.sn));
+    o.w = f32(r.w);
+    o.type = type;
+    o.idx64 = idx64;
+    const double e = r.eps;
+    const double near_r = div(r.b0, mul(2., kTau));
+    o.rnear2 = f32(mul(near_r, near_r));
+    if (type == 5) {
+        o.cx1 = f32(sub(1., e));
+        o.icx1 = f32(add(1., e));
+        o.kpre = f32(mul(mul(r.b0, sub(1., e)), add(1., e)));
+        o.ppre = f32(r.b0);
+        return;
+    }
+    const double sqe = sqr(e);
+    const double cx1 = div(sub(1., e), add(1., e));
+    const double ci = div(mul(0.5, sub(1., mul(e, e))), sqe);
+    const double t05 = (type == 81) ? div(r.rcut, sub(r.rcut, r.rc)) : 1.0;
+    o.s2 = f32(mul(2., sqe));
+    o.cx1 = f32(cx1);
+    o.icx1 = f32(div(1., cx1));
+    o.cxi = f32(div(1., mul(add(1., e), add(1., e))));
+    o.cyi = f32(div(1., mul(sub(1., e), sub(1., e))));
+    o.ome2 = f32(div(1., sub(1., mul(e, e))));
+    o.e4 = f32(mul(4., e));
+    o.cpi = f32(add(cx1, div(1., cx1)));
+    o.rc = f32(r.rc);
+    o.rcut = f32(r.rcut);
+    o.drs = f32(sub(r.rc, r.rcut));
+    o.dr2 = f32(mul(sub(r.rc, r.rcut), add(r.rc, r.rcut)));
+    o.rc2 = f32(mul(r.rc, r.rc));
+    o.rcut2 = f32(mul(r.rcut, r.rcut));
+    o.s2rc = f32(mul(mul(2., sqe), r.rc));
+    o.s2rcut = f32(mul(mul(2., sqe), r.rcut));
+    o.gpre = f32(mul(mul(mul(0.5, ci), r.b0), t05));
+    o.kpre = f32(type == 81 ? mul(mul(-0.5, r.b0), t05) : mul(0.5, r.b0));
+    o.ppre = f32(mul(mul(ci, r.b0), t05));
+    o.e1 = f32(div(mul(2., sqe), sub(1., e)));
+    o.e2 = f32(div(mul(2., sqe), add(1., e)));
+    const double sr = type == 81 ? r.rcut : r.rc;
+    o.singv = f32(mul(mul(2., sr), sqe));
+    const double srad = mul(add(kSingFrac, mul(kSingEps, e)), sr);
+    o.sing_r2 = f32(mul(srad, srad));
+    o.core_r2 = f32(mul(mul(kCoreFrac, r.rc), mul(kCoreFrac, r.rc)));
+}
+
+} // namespace pk
+} // namespace lt

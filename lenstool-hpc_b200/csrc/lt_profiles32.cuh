@@ -41,6 +41,13 @@ struct alignas(16) lt_rec32 {
 };
 static_assert(sizeof(lt_rec32) == 160, "record size");
 
+namespace lt {
+/* rnear2 of an FP64 proxy record: a halo of the FP32 class whose parameters, after an
+ * in-place update, need FP64 everywhere.  Every pixel then falls in its fallback region,
+ * and its potential terms are taken in FP64 as well. */
+constexpr float kProxy64 = __builtin_huge_valf();
+} // namespace lt
+
 #ifdef __CUDACC__
 namespace lt {
 

@@ -285,3 +285,31 @@ class RefLib:
                             C.byref(found), nf.ctypes.data_as(_ip), _d(fx), _d(fy))
         return {"chi2": chi.value, "images_found": found.value, "nfound": nf, "fx": fx.reshape(ns, 20),
                 "fy": fy.reshape(ns, 20)}
+
+    def bayes_rows(self, model, nhalos, free_flags, n_z_param, potfiles, pot_free, rows):
+        """The reference's module_readParameters_setbayesmapmodels over `rows` in turn:
+        halos 0..nhalos-1 are parameter-file halos (free_flags nhalos x 9 in the order
+        x, y, epot, emass, theta, rcore, vdisp, rcut, z), the rest potfile galaxies, potfile
+        after potfile.  Returns {x, y, b0, epot, cos, sin, rcore, rcut}, each nrows x ntot."""
+        L = self.lib
+        L.ltref_bayes_rows.argtypes = [C.c_int, C.c_int, _ip] + [_dp] * 9 + [_ip, C.c_int, C.c_int, _dp, _ip,
+                                                                              C.c_int, C.c_int, _dp, _dp]
+        t, x, y, ep, em, th, rc, vd, rcut, mag = model.arrays()
+        ntot = model.n
+        if mag is None:
+            mag = np.zeros(ntot)
+        ff = np.ascontiguousarray(free_flags, np.int32).reshape(nhalos, 9)
+        pp = np.ascontiguousarray([[p.count, p.mag0, p.sigma, p.cut, p.core, p.vdslope, p.slope] for p in potfiles],
+                                  np.float64).reshape(-1, 7)
+        pfree = np.ascontiguousarray(pot_free, np.int32).reshape(-1, 2)
+        rows = np.ascontiguousarray(rows, np.float64)
+        nrows, nparam = rows.shape
+        out = np.zeros((nrows, 8, ntot))
+        st = L.ltref_bayes_rows(nhalos, ntot, t.ctypes.data_as(_ip), *[_d(a) for a in (x, y, ep, em, th, rc, vd, rcut,
+                                                                                       mag)],
+                                ff.ctypes.data_as(_ip), n_z_param, len(potfiles), _d(pp), pfree.ctypes.data_as(_ip),
+                                nparam, nrows, _d(rows), _d(out))
+        if st:
+            raise RuntimeError(f"ltref_bayes_rows: {st}")
+        keys = ("x", "y", "b0", "epot", "cos", "sin", "rcore", "rcut")
+        return {k: out[:, i, :] for i, k in enumerate(keys)}

@@ -13,6 +13,8 @@
  *   - amplif_grid_CPU mode 5 (src/grid_amplif_CPU.cpp:38-84);
  *   - delense_barycenter (src/delense_CPU.cpp:6-140) and chi_computation
  *     (src/chi_computation.cpp:11-195), the strong-lensing chi2 by barycentric delensing;
+ *   - module_readParameters_setbayesmapmodels (src/module_readParameters.cpp:132-227) with
+ *     setScalingRelations and the potential-parameter step, a bayes.dat row's update;
  *   - the GPU kernels module_potential_totalPotential_SOA_GPU (src/potential_GPU.cu:139-187),
  *     module_potentialDerivatives_totalGradient2_SOA_GPU (src/gradient2_GPU.cu:337-398) and
  *     module_potentialDerivatives_Kmap_SOA_GPU (src/gradient2_GPU.cu:455-522), compiled as
@@ -299,6 +301,132 @@ int ltref_chi2(SOA_ARGS, double xmin, double xmax, double ymin, double ymax, int
         for (int k = 0; k < numfound[s] && k < MAXIMPERSOURCE; k++) {
             fx[s * MAXIMPERSOURCE + k] = pos[(size_t)s * MAXIMPERSOURCE + k].x;
             fy[s * MAXIMPERSOURCE + k] = pos[(size_t)s * MAXIMPERSOURCE + k].y;
+        }
+    }
+    return 0;
+}
+
+} // extern "C"
+
+/* ---- bayes.dat rows: module_readParameters_setbayesmapmodels ------------------------ */
+
+#include <float.h>
+
+#include "module_readParameters.hpp"
+
+/* module_readParameters.cpp needs the observer distance only for potfile lengths given
+ * in kpc, which these calls never pass (the GSL-based cosmology module is absent). */
+type_t module_cosmodistances_observerObject(type_t, cosmo_param) { abort(); }
+
+extern "C" {
+
+/* The reference's own per-row update (src/module_readParameters.cpp:132-227, with
+ * setScalingRelations :1539-1656 and the potential-parameter step :2873-2936) applied to
+ * rows 0..nrows-1 in turn.  Halos 0..nhalos-1 are the parameter-file halos (SOA_index =
+ * identity), halos nhalos..ntot-1 the potfile galaxies, potfile after potfile.  The model
+ * state is first taken to the fixed point of the potential-parameter step (three passes
+ * of the reference's function).  free_flags: nhalos x 9 in the order x, y, epot, emass,
+ * theta, rcore, vdisp, rcut, z; pot_params: npot x 7 (count, mag0, sigma, cut, core,
+ * vdslope, slope); pot_free: npot x 2 (ircut, isigma).  out: nrows x 8 x ntot (x, y, b0,
+ * epot, cos, sin, rcore, rcut). */
+int ltref_bayes_rows(int nhalos, int ntot, const int *type, const double *x, const double *y, const double *epot,
+                     const double *emass, const double *theta, const double *rcore, const double *vdisp,
+                     const double *rcut, const double *mag, const int *free_flags, int n_z_param, int npot,
+                     const double *pot_params, const int *pot_free, int nparam, int nrows, const double *rows,
+                     double *out)
+{
+    if (npot > N_MAX_POTFILE) return -1;
+    std::vector<int> t(type, type + ntot), soa_index((size_t)ntot);
+    std::vector<double> f[16];
+    for (auto &v : f) v.assign((size_t)ntot, 0.);
+    Potential_SOA L;
+    memset(&L, 0, sizeof(L));
+    L.type = t.data();
+    L.position_x = f[0].data();
+    L.position_y = f[1].data();
+    L.b0 = f[2].data();
+    L.vdisp = f[3].data();
+    L.ellipticity_angle = f[4].data();
+    L.ellipticity = f[5].data();
+    L.ellipticity_potential = f[6].data();
+    L.rcore = f[7].data();
+    L.rcut = f[8].data();
+    L.z = f[9].data();
+    L.mag = f[10].data();
+    L.anglecos = f[11].data();
+    L.anglesin = f[12].data();
+    L.dlsds = f[13].data();
+    L.SOA_index = soa_index.data();
+    for (int i = 0; i < ntot; i++) {
+        soa_index[i] = i;
+        L.position_x[i] = x[i];
+        L.position_y[i] = y[i];
+        L.vdisp[i] = vdisp[i];
+        L.ellipticity_angle[i] = theta[i];
+        L.ellipticity[i] = emass[i];
+        L.ellipticity_potential[i] = epot[i];
+        L.rcore[i] = rcore[i];
+        L.rcut[i] = rcut[i];
+        L.mag[i] = mag ? mag[i] : 0.;
+        L.anglecos[i] = cos(theta[i]);
+        L.anglesin[i] = sin(theta[i]);
+    }
+    for (int it = 0; it < 3; it++)
+        for (int i = 0; i < ntot; i++) module_readParameters_calculatePotentialparameter_SOA(&L, i);
+    runmode_param rm = runmode_param();
+    rm.nhalos = nhalos;
+    rm.n_tot_halos = ntot;
+    rm.N_z_param = n_z_param;
+    rm.potfile = npot > 0;
+    rm.Nb_potfile = npot;
+    cosmo_param cosmo;
+    memset(&cosmo, 0, sizeof(cosmo));
+    std::vector<potentialoptimization> lim((size_t)(nhalos > 0 ? nhalos : 1));
+    memset(lim.data(), 0, sizeof(potentialoptimization) * lim.size());
+    for (int i = 0; i < nhalos; i++) {
+        const int *fl = free_flags + 9 * i;
+        lim[i].position.x.block = fl[0];
+        lim[i].position.y.block = fl[1];
+        lim[i].ellipticity_potential.block = fl[2];
+        lim[i].ellipticity.block = fl[3];
+        lim[i].ellipticity_angle.block = fl[4];
+        lim[i].rcore.block = fl[5];
+        lim[i].vdisp.block = fl[6];
+        lim[i].rcut.block = fl[7];
+        lim[i].z.block = fl[8];
+    }
+    std::vector<potfile_param> pf((size_t)(npot > 0 ? npot : 1));
+    memset(pf.data(), 0, sizeof(potfile_param) * pf.size());
+    for (int k = 0; k < npot; k++) {
+        const double *q = pot_params + 7 * k;
+        potfile_param &p = pf[k];
+        p.ftype = 1;
+        p.npotfile = (int)q[0];
+        rm.npotfile[k] = p.npotfile;
+        p.mag0 = q[1];
+        p.sigma1 = q[2];
+        p.cut1 = q[3];
+        p.cutkpc1 = DBL_MAX;
+        p.core = q[4];
+        p.corekpc = -1;
+        p.vdslope1 = q[5];
+        p.slope1 = q[6];
+        p.ircut = pot_free[2 * k];
+        p.isigma = pot_free[2 * k + 1];
+    }
+    std::vector<double> bayespot(rows, rows + (size_t)nrows * nparam);
+    for (int r = 0; r < nrows; r++) {
+        module_readParameters_setbayesmapmodels(&rm, &cosmo, lim.data(), pf.data(), &L, bayespot.data(), nparam, r);
+        double *o = out + (size_t)r * 8 * ntot;
+        for (int i = 0; i < ntot; i++) {
+            o[0 * ntot + i] = L.position_x[i];
+            o[1 * ntot + i] = L.position_y[i];
+            o[2 * ntot + i] = L.b0[i];
+            o[3 * ntot + i] = L.ellipticity_potential[i];
+            o[4 * ntot + i] = L.anglecos[i];
+            o[5 * ntot + i] = L.anglesin[i];
+            o[6 * ntot + i] = L.rcore[i];
+            o[7 * ntot + i] = L.rcut[i];
         }
     }
     return 0;
