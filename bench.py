@@ -5,7 +5,8 @@ over 300"x300" for the seeded 1000-halo catalogue (4 cluster-scale + 996 galaxy-
 cut-dPIE halos), computed by the fused lens-maps kernel (LT_FP32C by default).  Metric:
 halo x pixel evaluations per second, counting the Hessian and the potential sum once each
 per (halo, pixel) pair.  The same JSON line also carries LT_FP64 on the same step, the
-posterior-batch workload (maps/s against one map call per set), the serving workload
+posterior-batch workload (bayes rows applied on the device + one batch launch; maps/s
+against the reference's loop of one launch per map and set), the serving workload
 (p50/p99 latency, maps/s against one plain call per request) and the delensing + chi2
 workload (models/s against the reference's CPU code).
 
@@ -159,54 +160,79 @@ def _percentile(xs, q):
     return float(np.percentile(np.asarray(xs, np.float64), q)) if len(xs) else None
 
 
-def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sample=16, e2e=True):
-    """Posterior-batch workload: n_sets Gaussian 5% perturbations (seeded) of the 200-halo
-    catalogue (2 cluster + 198 galaxy halos), each on a grid drawn from {512^2, 1024^2,
-    2048^2} over the 200"x200" field; outputs mu and kappa per set; all sets in one
-    graph-captured persistent launch (lt_batch).  Compared with one map call per set in
-    the reference's calling pattern (upload, compute, copy back, release)."""
+def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sample=48, e2e=True):
+    """Posterior-batch workload: n_sets bayes.dat-style rows (seeded Gaussian 5% perturbations
+    of every halo's x, y, emass, theta, rcore, vdisp, rcut) of the 200-halo model (2 cluster
+    + 198 galaxy halos), each on a grid drawn from {512^2, 1024^2, 2048^2} over the
+    200"x200" field; outputs mu and kappa per set.  One step: the rows (resident in HBM)
+    applied to the sets' resident catalogues (lt_bayes_apply, one launch) and all sets in
+    one graph-captured persistent launch (lt_batch).  Compared with the reference's
+    bayes-map loop: one launch per map and set (upload, compute, copy back, release)."""
     import torch
     lt = _package()
-    from lenstool_hpc_b200 import catalog
+    from lenstool_hpc_b200 import bayes, catalog
     rng = np.random.Generator(np.random.PCG64(20261203 + 2))
-    base = catalog.cluster_galaxy_catalog(2, 198, 20261203)
+    model = bayes.model_from_parameters(catalog.cluster_galaxy_parameters(2, 198, 20261203))
+    B = bayes
+    cols = bayes.columns_from_free([{B.X, B.Y, B.EMASS, B.THETA, B.RCORE, B.VDISP, B.RCUT}] * model.n)
     sizes = rng.choice([512, 1024, 2048], n_sets)
-    sets = [catalog.perturb_catalog(base, rng) for _ in range(n_sets)]
+    rows = bayes.synthetic_rows(model, cols, n_sets, rng)
+    base = bayes.catalog_from_state(model, bayes.base_state(model))
     grids = {n: catalog.Grid.square(100., int(n)) for n in (512, 1024, 2048)}
     dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
     D = dls / dos
     kinds = ("mu", "kappa")
-    cats = [ctx.upload(c) for c in sets]
+    cats = [ctx.upload(base) for _ in range(n_sets)]
+    post = ctx.bayes(model, cols)
+    rows_dev = torch.tensor(rows, device="cuda")
     outs = [{k: torch.empty((int(n), int(n)), dtype=torch.float64, device="cuda") for k in kinds} for n in sizes]
     reqs = [lt.Request(c, grids[int(n)], o, dlsds=D) for c, n, o in zip(cats, sizes, outs)]
     batch = ctx.batch(reqs, precision=precision)
     evals = float(sum(int(n) * int(n) for n in sizes)) * base.n
     stream = torch.cuda.Stream()
     for _ in range(warmup):
+        post.apply(rows_dev, cats, stream)
         batch.launch(stream)
     ctx.synchronize(stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n0 = lt.launch_count()
     e0.record(stream)
     for _ in range(steps):
+        post.apply(rows_dev, cats, stream)
         batch.launch(stream)
     e1.record(stream)
     ctx.synchronize(stream)
     launches = lt.launch_count() - n0
     dt = e0.elapsed_time(e1) / 1e3 / steps
-    res = {"workload": f"posterior_batch: {n_sets} sets x {base.n} halos, grids U{{512,1024,2048}}^2, mu+kappa",
-           "precision": precision, "maps_per_s": 2 * n_sets / dt, "sets_per_s": n_sets / dt, "evals_per_s": evals / dt,
-           "ms_per_step": dt * 1e3, "gpu_launches_per_step": launches / steps,
-           "evals_per_step": evals, "l2": f"outputs {2 * 8 * evals / base.n / 1e9:.1f} GB per step > L2"}
-    # one map call per set (upload, compute into pageable host arrays, release): a sample
-    # of the sets, scaled to all sets by their halo x pixel evaluations
-    plain = {}
+    res = {"workload": f"posterior_batch: {n_sets} bayes rows x {base.n} halos, grids U{{512,1024,2048}}^2, "
+                       f"mu+kappa", "precision": precision, "maps_per_s": 2 * n_sets / dt, "sets_per_s": n_sets / dt,
+           "evals_per_s": evals / dt, "ms_per_step": dt * 1e3, "gpu_launches_per_step": launches / steps,
+           "evals_per_step": evals, "l2": f"outputs {2 * 8 * evals / base.n / 1e9:.1f} GB per step > L2",
+           "step": "lt_bayes_apply of the rows (HBM) + one lt_batch graph"}
+    # the sets as host catalogues (the reference's host-side row update), for the plain loop
+    sets = [bayes.catalog_from_state(model, bayes.reference_state(model, (), cols, rows[i]))
+            for i in range(plain_sample)]
+    # the reference's bayes-map loop (utils/maps/main.cpp:428-587): one launch per map and
+    # set, each with its own upload, Hessian sum, copy back to pageable host memory and
+    # release; a sample of the sets, scaled to all sets by their halo x pixel evaluations.
+    # Also timed: both maps from one call per set (the fused epilogue, same Hessian sum).
+    plain, fused = {}, {}
     idx = list(range(plain_sample))
+    sample_evals = float(sum(int(sizes[i]) ** 2 for i in idx)) * base.n
     for prec in ("fp64", precision):
         host = {i: {k: np.empty((int(sizes[i]), int(sizes[i]))) for k in kinds} for i in idx}
         c = ctx.upload(sets[0])
         ctx.hessian_maps(c, grids[int(sizes[0])], list(kinds), precision=prec, dlsds=D, out=list(host[0].values()))
         c.release()
+        t0 = time.perf_counter()
+        for k in kinds:
+            for i in idx:
+                c = ctx.upload(sets[i])
+                ctx.hessian_maps(c, grids[int(sizes[i])], [k], precision=prec, dlsds=D, out=[host[i][k]])
+                c.release()
+        t = time.perf_counter() - t0
+        plain[prec] = {"maps_per_s": 2 * n_sets / (t * evals / sample_evals), "sample_sets": len(idx),
+                       "sample_s": t}
         t0 = time.perf_counter()
         for i in idx:
             c = ctx.upload(sets[i])
@@ -214,12 +240,12 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
                              out=list(host[i].values()))
             c.release()
         t = time.perf_counter() - t0
-        sample_evals = float(sum(int(sizes[i]) ** 2 for i in idx)) * base.n
-        t_all = t * evals / sample_evals
-        plain[prec] = {"maps_per_s": 2 * n_sets / t_all, "sample_sets": len(idx), "sample_s": t}
-    res["one_map_per_call"] = plain
-    res["speedup_vs_one_map_per_call_fp64"] = res["maps_per_s"] / plain["fp64"]["maps_per_s"]
-    res["speedup_vs_one_map_per_call_same_precision"] = res["maps_per_s"] / plain[precision]["maps_per_s"]
+        fused[prec] = {"maps_per_s": 2 * n_sets / (t * evals / sample_evals), "sample_s": t}
+    res["one_map_per_launch"] = plain
+    res["two_maps_per_call"] = fused
+    res["speedup_vs_one_map_per_launch_fp64"] = res["maps_per_s"] / plain["fp64"]["maps_per_s"]
+    res["speedup_vs_one_map_per_launch_same_precision"] = res["maps_per_s"] / plain[precision]["maps_per_s"]
+    res["speedup_vs_two_maps_per_call_fp64"] = res["maps_per_s"] / fused["fp64"]["maps_per_s"]
     try:
         import psutil
         host_free = psutil.virtual_memory().available
@@ -229,10 +255,10 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
         res["e2e"] = {"skipped": f"host memory available {host_free / 1e9:.0f} GB < 3x the maps"}
         e2e = False
     if e2e:
-        # end to end through the public API: every set's catalogue uploaded from host arrays
-        # and every map delivered to (pinned) host memory, through the serving loop, which
-        # copies finished sets out while later ones compute.  The host buffers and the
-        # server are set up outside the timed region.
+        # end to end through the public API: the rows from host memory applied to the
+        # resident catalogues (lt_bayes_apply), every set served by the serving loop with its
+        # maps delivered to pinned host memory while later sets compute.  The catalogue
+        # slots, the host buffers and the server are set up outside the timed region.
         batch.destroy()
         batch = None
         host = [{k: torch.empty((int(n), int(n)), dtype=torch.float64, pin_memory=True) for k in kinds}
@@ -241,22 +267,25 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
             srv.wait(srv.submit(lt.Request(cats[0], grids[512], {"kappa": host[0]["kappa"][:512, :512].contiguous()},
                                            dlsds=D)))
             t0 = time.perf_counter()
-            cats2 = [ctx.upload(c) for c in sets]
-            tickets = [srv.submit(lt.Request(c, grids[int(n)], h, dlsds=D)) for c, n, h in zip(cats2, sizes, host)]
+            post.apply(rows, cats)
+            ctx.synchronize()
+            tickets = [srv.submit(lt.Request(c, grids[int(n)], h, dlsds=D)) for c, n, h in zip(cats, sizes, host)]
             for t in tickets:
                 srv.wait(t, 3600.)
             te = time.perf_counter() - t0
             for t in tickets:
                 srv.release(t)
-        for c in cats2:
-            c.release()
-        res["e2e"] = {"maps_per_s": 2 * n_sets / te, "h2d_bytes_per_step": n_sets * base.n * (192 + 160),
+        ntheta = int(np.sum(cols[:, 0] == bayes.THETA))
+        res["e2e"] = {"maps_per_s": 2 * n_sets / te,
+                      "h2d_bytes_per_step": int(rows.nbytes + n_sets * (16 * ntheta + 24)),
                       "d2h_bytes_per_step": int(2 * 8 * evals / base.n),
-                      "note": "upload of every set's catalogue + every set served (lt_server) with its maps "
-                              "copied to pinned host memory while later sets compute"}
-        res["e2e"]["speedup_vs_one_map_per_call_fp64"] = res["e2e"]["maps_per_s"] / plain["fp64"]["maps_per_s"]
+                      "note": "bayes rows from host memory applied on the device (lt_bayes_apply) + every set "
+                              "served (lt_server) with its maps copied to pinned host memory while later sets "
+                              "compute"}
+        res["e2e"]["speedup_vs_one_map_per_launch_fp64"] = res["e2e"]["maps_per_s"] / plain["fp64"]["maps_per_s"]
     if batch is not None:
         batch.destroy()
+    post.destroy()
     for c in cats:
         c.release()
     return res
