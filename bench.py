@@ -16,7 +16,9 @@ workload (models/s against the reference's CPU code).
 
 --impl reference times the reference's own CPU code (oracle/_ref: gradient2_grid_CPU and
 the reference potential kernel compiled for the host) on all host cores, on a bounded
-band of rows of the same workload.  Multi-GPU (torchrun): independent replicas, one per
+band of rows of the same workload; its line also carries `reference_gpu`, the reference's
+own GPU kernels built for sm_100a (type_t double and float) timed on the full workload on
+this GPU.  Multi-GPU (torchrun): independent replicas, one per
 GPU (the maps are independent; no collective on the data path); value = all ranks' evals
 / max-over-ranks time.
 """
@@ -154,6 +156,45 @@ def reference_cpu(steps, warmup, rows=None):
               f"kernel on the host), {threads} OpenMP threads")
     return v, {"value": v, "unit": "evals/s", "cores": threads, "kind": "reference", "sample": sample,
                "seconds_per_sample": float(np.mean(times))}
+
+
+def reference_gpu(reps=1, band_rows=32):
+    """The reference's own GPU kernels (src/gradient2_GPU.cu, src/potential_GPU.cu, built
+    for sm_100a from its sources, type_t = double and float) on the full workload, one
+    Hessian and one potential launch per step as its wrappers make them (32 x 16 threads,
+    one pixel per thread); evals counted as for `value`.  Each build's error is measured
+    against the reference CPU FP64 code on a band of rows."""
+    import oracle
+    from lenstool_hpc_b200 import catalog
+    cat, g = catalog.workload(WORKLOAD)
+    band = catalog.Grid(g.xmin, g.xmax, g.ymin, g.ymax, g.nx, band_rows, 0, g.ny // 2, dx=g.dx, dy=g.dy)
+    bgrid = catalog.Grid(g.xmin, g.xmax, g.ymin + (g.ny // 2) * g.dy, g.ymax, g.nx, band_rows, dx=g.dx, dy=g.dy)
+    cpu_h = cpu_p = None
+    out = {"workload": WORKLOAD, "launch": "reference kernels, 32x16 threads, one pixel per thread"}
+    for build in ("fp64", "fp32"):
+        try:
+            lib = oracle.RefGpuLib(build)
+            th, _ = lib.grid("hessian", cat, g, reps=reps, want=False)
+            tp, _ = lib.grid("potential", cat, g, reps=reps, want=False)
+            _, h = lib.grid("hessian", cat, bgrid, reps=1)
+            _, p = lib.grid("potential", cat, bgrid, reps=1)
+        except (FileNotFoundError, RuntimeError, OSError) as ex:
+            out[build] = {"unavailable": str(ex)}
+            continue
+        if cpu_h is None:
+            ref = oracle.RefLib()
+            cpu_h = ref.hess_grid(cat, band)
+            px, py = band.coords()
+            cpu_p = ref.pot81_points(cat, px, py).reshape(band_rows, g.nx)
+
+        def err(a, b):
+            rms = np.sqrt(np.mean(b * b))
+            return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), rms)))
+        evals = 2. * g.nx * g.ny * cat.n
+        out[build] = {"hessian_ms": th, "potential_ms": tp, "evals_per_s": evals / ((th + tp) / 1e3),
+                      "max_rel_err_vs_reference_cpu_fp64": {"hessian": max(err(h[k], cpu_h[k]) for k in range(4)),
+                                                            "potential": err(p[0], cpu_p)}}
+    return out
 
 
 def _percentile(xs, q):
@@ -429,6 +470,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="--impl reference: skip timing the reference's GPU kernels beside its CPU code")
     ap.add_argument("--grid", type=int, default=0, help="smaller square grid (profiling cases)")
     ap.add_argument("--maps", default="all", choices=["all", "hessian", "potential"],
                     help="all = kappa/gamma1/gamma2/mu/psi (the workload); the others time one sum")
@@ -455,6 +498,11 @@ def main():
                 "impl": "reference", "config": {"workload": WORKLOAD, "sample": info["sample"]},
                 "cpu_baseline": info, "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0,
                                               "d2h_bytes_per_step": 0}}
+        if not args.no_reference_gpu:
+            try:
+                line["reference_gpu"] = reference_gpu()
+            except Exception as ex:  # no device here: the CPU arm stands alone
+                line["reference_gpu"] = {"unavailable": str(ex)}
         print(json.dumps(line))
         return 0
 

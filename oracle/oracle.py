@@ -313,3 +313,35 @@ class RefLib:
             raise RuntimeError(f"ltref_bayes_rows: {st}")
         keys = ("x", "y", "b0", "epot", "cos", "sin", "rcore", "rcut")
         return {k: out[:, i, :] for i, k in enumerate(keys)}
+
+
+REF_GPU_SO = {"fp64": HERE / "_ref" / "libltref_gpu.so", "fp32": HERE / "_ref" / "libltref_gpu32.so"}
+
+
+class RefGpuLib:
+    """The reference's own GPU kernels (src/gradient2_GPU.cu, src/potential_GPU.cu) built
+    for sm_100a: type_t = double ("fp64") or float ("fp32", the reference's default)."""
+
+    def __init__(self, build="fp64"):
+        path = REF_GPU_SO[build]
+        if not path.exists():
+            raise FileNotFoundError(f"{path} not built (oracle/Makefile target 'ref')")
+        self.build = build
+        self.lib = C.CDLL(str(path))
+        self.lib.ltrefgpu_grid.argtypes = [C.c_int, C.c_int, _ip] + [_dp] * 8 + [C.c_double] * 4 + [C.c_int] * 3 + [
+            _dp, _dp]
+
+    def grid(self, which, cat, g, reps=1, want=True):
+        """which 'hessian' (planes a, b, c, d) or 'potential'; returns (ms per launch, planes)."""
+        w = {"hessian": 0, "potential": 1}[which]
+        t = np.ascontiguousarray(cat.type, np.int32)
+        fl = [np.ascontiguousarray(getattr(cat, f), np.float64) for f in (
+            "position_x", "position_y", "anglecos", "anglesin", "ellipticity_potential", "rcore", "rcut", "b0")]
+        npl = 4 if w == 0 else 1
+        out = np.empty((npl, g.ny, g.nx)) if want else None
+        ms = C.c_double()
+        st = self.lib.ltrefgpu_grid(w, int(t.size), t.ctypes.data_as(_ip), *[_d(a) for a in fl], g.xmin, g.ymin,
+                                    g.dx, g.dy, g.nx, g.ny, reps, C.byref(ms), _d(out) if want else None)
+        if st:
+            raise RuntimeError(f"ltrefgpu_grid: status {st}")
+        return ms.value, out
