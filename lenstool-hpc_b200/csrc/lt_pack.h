@@ -197,6 +197,8 @@ LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     o.ppre = f32(mul(mul(ci, r.b0), t05));
     o.e1 = f32(div(mul(2., sqe), sub(1., e)));
     o.e2 = f32(div(mul(2., sqe), add(1., e)));
+    o.irc = f32(div(1., r.rc));
+    o.ircut = f32(div(1., r.rcut));
     const double sr = type == 81 ? r.rcut : r.rc;
     o.singv = f32(mul(mul(2., sr), sqe));
     const double srad = mul(add(kSingFrac, mul(kSingEps, e)), sr);

@@ -35,8 +35,8 @@ struct alignas(16) lt_rec32 {
     float gpre, rc, rcut, drs;    /* gamma prefactor, rc, rcut, rc - rcut                    */
     float dr2, rc2, rcut2, w;     /* rc^2 - rcut^2, rc^2, rcut^2, Kmap weight                */
     float rnear2, singv, sing_r2, core_r2; /* FP64 fallback regions (squared radii)          */
-    float cpi, s2rc, s2rcut, pad; /* cx1 + 1/cx1, 2 sqrt(e) rc, 2 sqrt(e) rcut                */
-    float e1, e2, ppre, pad2;     /* potential: 2 sqrt(e)/(1-e), 2 sqrt(e)/(1+e), prefactor   */
+    float cpi, s2rc, s2rcut, irc; /* cx1 + 1/cx1, 2 sqrt(e) rc, 2 sqrt(e) rcut, 1/rc           */
+    float e1, e2, ppre, ircut;    /* potential: 2 sqrt(e)/(1-e), 2 sqrt(e)/(1+e), prefactor, 1/rcut */
     int32_t type, idx64, pad0, pad1;
 };
 static_assert(sizeof(lt_rec32) == 160, "record size");
@@ -52,6 +52,39 @@ constexpr float kProxy64 = __builtin_huge_valf();
 namespace lt {
 
 __device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+
+/* Square root to the approximate instruction's accuracy (relative error ~2^-23), for
+ * operands whose rounding the compensated path tolerates; zero and denormals give 0. */
+__device__ __forceinline__ float fsqrt(float x)
+{
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+/* atan2 in FP32.  a = min(|x|,|y|)/max(|x|,|y|) in [0, 1]; atan a = a P(a^2) with P of
+ * degree 7, fitted to atan(a)/a on [0, 1] by a Remez exchange on the relative error
+ * (max 9.9e-8 in exact arithmetic); then atan2 = pi/2 - atan a where |y| > |x|,
+ * pi - that where x < 0, with the sign of y.  Against FP64 atan2: <= 3.8e-7 absolute,
+ * 3e-7 relative (checked over |x|, |y| in [1e-6, 1e3]).  Needs (x, y) != (0, 0). */
+__device__ __forceinline__ float fatan2(float y, float x)
+{
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float a = fminf(ax, ay) * frcp(fmaxf(ax, ay));
+    const float s = a * a;
+    float p = -4.693276249e-03f;
+    p = fmaf(p, s, 2.425240353e-02f);
+    p = fmaf(p, s, -5.948639289e-02f);
+    p = fmaf(p, s, 9.914293140e-02f);
+    p = fmaf(p, s, -1.401948035e-01f);
+    p = fmaf(p, s, 1.996972412e-01f);
+    p = fmaf(p, s, -3.333199024e-01f);
+    p = fmaf(p, s, 9.999998808e-01f);
+    float r = a * p;
+    r = ay > ax ? 1.57079637f - r : r;
+    r = x < 0.f ? 3.14159274f - r : r;
+    return copysignf(r, y);
+}
 
 struct KG32 {
     float k, g1, g2; /* halo-frame convergence and shear */
@@ -187,41 +220,55 @@ __device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
     return {h.ppre * li, -h.ppre * lr};
 }
 
-/* Potential, FP32.  pi05 of src/potential_GPU.cu:47-72 evaluated through identities that
- * remove its transcendental functions except the two complex logarithms per radius:
- *   exp(eta_re) = exp(-asinh(s)/2) = (|s| + sqrt(s^2 + 1))^(-sign(s)/2),  s = e1 v/z,
- *   eta_im = asin(t)/2, t = e2 u/z:  sin 2eta_im = t, cos 2eta_im = sqrt(1 - t^2),
- *     cos eta_im = sqrt((1 + cos 2eta_im)/2), sin eta_im = t/(2 cos eta_im),
- *   exp(zeta) = sqrt(ratio), ratio = (sqrt(rho^2) + sqrt(r^2 + rho^2))/r,
- *   sinh(2 zeta) = (ratio - 1/ratio)/2.
+/* Potential, FP32.  pi05 of src/potential_GPU.cu:47-72 is, with b1 = cosh(eta + zeta),
+ * b2 = cosh(eta - zeta) (zeta real), r (Im k u - Re k v) b0 ci/rho_e with
+ *   k = sinh(2 eta) log(cosh^2 eta/(b1 b2)) + sinh(2 zeta) log(b1/b2).
+ * Writing w = tanh eta tanh zeta and a = eta_re,
+ *   b1 b2 = cosh^2 eta cosh^2 zeta (1 - w)(1 + w),   b1/b2 = (1 + w)/(1 - w),
+ *   1 +- w = N+- / (cosh 2a + cos 2 eta_im),
+ *   N+  = (e^{2a}  - 2 sinh 2a/(rho + 1) + cos 2 eta_im) + i B,
+ *   N-  = (e^{-2a} + 2 sinh 2a/(rho + 1) + cos 2 eta_im) - i B,   B = tanh zeta sin 2 eta_im,
+ * whose real parts are sums of positive terms or lose at most half (no cancellation, also
+ * where tanh eta -> +-1 at high ellipticity), so
+ *   log(b1/b2) = log|N+|^2/|N-|^2 / 2 + i arg(N+ conj N-),
+ *   log(cosh^2 eta/(b1 b2)) = -log(cosh^4 zeta |N+|^2 |N-|^2/(cosh 2a + cos 2 eta_im)^4)/2
+ *                             - i arg(N+ N-),
+ * with Re(N+ N-) = Re N+ Re N- + B^2 > 0 and Im(N+ N-) = -2 B tanh zeta sinh 2a exactly;
+ * the arguments are those of the reference's principal logarithms (both |arg| < pi), and no
+ * complex quotient is formed.  With s = e1 v/z and t = e2 u/z:
+ *   e^{2a} = exp(-asinh s) = (|s| + sqrt(s^2 + 1))^(-sign s),
+ *   sin 2 eta_im = t, cos 2 eta_im = sqrt(1 - t^2),
+ *   e^{2 zeta} = rho = (rho_e + sqrt(r^2 + rho_e^2))/r, with rho - 1 taken without
+ *   cancellation as (rho_e + rho_e^2/(sqrt(r^2 + rho_e^2) + r))/r,
+ *   tanh zeta = (rho - 1)/(rho + 1), cosh^2 zeta = (rho + 1)^2/(4 rho),
+ *   sinh 2 zeta = (rho - 1)(rho + 1)/(2 rho).
  * Returns the halo's potential without the FP64 cluster terms; far from the halo the
  * core - cut difference loses ~1e-5 of the term, small against the map's scale. */
 struct Pi05Shared {
-    float E, iE, ce, se, c2e, t;  /* exp(eta_re)^{+-1}, cos/sin eta_im, cos/sin 2 eta_im */
-    float ch2r, ch2i;             /* cosh(eta)^2 */
-    float sh2r, sh2i;             /* sinh(2 eta) */
+    float sh2r, sh2i;      /* sinh(2 eta) */
+    float E2, iE2, sh2a;   /* e^{2a}, e^{-2a}, sinh 2a */
+    float c2e, t;          /* cos, sin of 2 eta_im */
+    float itd4;            /* (cosh 2a + cos 2 eta_im)^-4 */
 };
 
-__device__ __forceinline__ float clog_re2(float a, float b) { return 0.5f * __logf(a * a + b * b); }
-
 __device__ __forceinline__ float pi05_term32(const Pi05Shared &p, float u, float v, float srem, float rem2, float r,
-                                             float r2)
+                                             float r2, float ir)
 {
-    const float ratio = (srem + sqrtf(r2 + rem2)) * frcp(r);
-    const float Z = sqrtf(ratio);
-    const float iZ = frcp(Z);
-    const float ez = p.E * Z, iez = p.iE * iZ, ezm = p.E * iZ, iezm = p.iE * Z;
-    const float b1r = 0.5f * (ez + iez) * p.ce, b1i = 0.5f * (ez - iez) * p.se;
-    const float b2r = 0.5f * (ezm + iezm) * p.ce, b2i = 0.5f * (ezm - iezm) * p.se;
-    /* b1 b2 and the two quotients */
-    const float pr = b1r * b2r - b1i * b2i, pi = b1r * b2i + b1i * b2r;
-    const float ip = frcp(pr * pr + pi * pi);
-    const float q1r = (p.ch2r * pr + p.ch2i * pi) * ip, q1i = (p.ch2i * pr - p.ch2r * pi) * ip;
-    const float ib2 = frcp(b2r * b2r + b2i * b2i);
-    const float q2r = (b1r * b2r + b1i * b2i) * ib2, q2i = (b1i * b2r - b1r * b2i) * ib2;
-    const float a1r = clog_re2(q1r, q1i), a1i = atan2f(q1i, q1r);
-    const float a2r = clog_re2(q2r, q2i), a2i = atan2f(q2i, q2r);
-    const float sh2z = 0.5f * (ratio - frcp(ratio));
+    const float q = fsqrt(r2 + rem2);
+    const float dm = (srem + rem2 * frcp(q + r)) * ir; /* rho - 1 */
+    const float rho = 1.f + dm, rho1 = rho + 1.f;
+    const float inv = frcp(rho * rho1);
+    const float irho = rho1 * inv, irho1 = rho * inv;
+    const float tz = dm * irho1;                        /* tanh zeta */
+    const float sh2z = 0.5f * dm * rho1 * irho;         /* sinh 2 zeta */
+    const float ch2z = 0.25f * rho1 * rho1 * irho;      /* cosh^2 zeta */
+    const float m = 2.f * irho1 * p.sh2a;
+    const float A = (p.E2 - m) + p.c2e, C = (p.iE2 + m) + p.c2e, B = tz * p.t, B2 = B * B;
+    const float np2 = A * A + B2, nm2 = C * C + B2;
+    const float a2r = 0.5f * __logf(np2 * frcp(nm2));
+    const float a2i = fatan2(B * (A + C), A * C - B2);
+    const float a1r = -0.5f * __logf((ch2z * ch2z) * (np2 * nm2) * p.itd4);
+    const float a1i = fatan2(2.f * B * tz * p.sh2a, A * C + B2);
     const float kr = (p.sh2r * a1r - p.sh2i * a1i) + sh2z * a2r;
     const float ki = (p.sh2i * a1r + p.sh2r * a1i) + sh2z * a2i;
     return r * (ki * u - kr * v);
@@ -230,30 +277,32 @@ __device__ __forceinline__ float pi05_term32(const Pi05Shared &p, float u, float
 template <int TYPE>
 __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v)
 {
-    if (TYPE == 5) return h.ppre * sqrtf(u * u * h.cx1 + v * v * h.icx1);
+    if (TYPE == 5) return h.ppre * fsqrt(u * u * h.cx1 + v * v * h.icx1);
     const float uu = u * u, vv = v * v;
     const float rem2 = uu * h.cxi + vv * h.cyi;
-    const float srem = sqrtf(rem2);
+    const float irem = rsqrtf(rem2);
+    const float srem = rem2 * irem;
     const float iz = rsqrtf(uu + vv);
-    Pi05Shared p;
     const float s = h.e1 * v * iz;
-    const float t = fabsf(s) + sqrtf(s * s + 1.f);
-    const float rt = rsqrtf(t), st = t * rt;
-    p.E = s >= 0.f ? rt : st;
-    p.iE = s >= 0.f ? st : rt;
-    p.t = h.e2 * u * iz;
-    p.c2e = sqrtf(fmaxf(1.f - p.t * p.t, 0.f));
-    p.ce = sqrtf(0.5f * (1.f + p.c2e));
-    p.se = 0.5f * p.t * frcp(p.ce);
-    const float chr = 0.5f * (p.E + p.iE) * p.ce, chi = 0.5f * (p.E - p.iE) * p.se;
-    p.ch2r = chr * chr - chi * chi;
-    p.ch2i = 2.f * chr * chi;
-    const float E2 = p.E * p.E, iE2 = p.iE * p.iE;
-    p.sh2r = 0.5f * (E2 - iE2) * p.c2e;
-    p.sh2i = 0.5f * (E2 + iE2) * p.t;
-    float term = pi05_term32(p, u, v, srem, rem2, h.rc, h.rc2);
-    if (TYPE == 81) term -= pi05_term32(p, u, v, srem, rem2, h.rcut, h.rcut2);
-    return h.ppre * term * frcp(srem);
+    const float t = h.e2 * u * iz;
+    const float g = fabsf(s) + fsqrt(s * s + 1.f);
+    const float ig = frcp(g);
+    const float E2 = s >= 0.f ? ig : g, iE2 = s >= 0.f ? g : ig; /* exp(+-2 eta_re) */
+    const float ch2a = 0.5f * (E2 + iE2), sh2a = 0.5f * (E2 - iE2);
+    const float c2e = fsqrt(fmaxf(1.f - t * t, 0.f));
+    Pi05Shared p;
+    p.sh2r = sh2a * c2e;
+    p.sh2i = ch2a * t;
+    p.E2 = E2;
+    p.iE2 = iE2;
+    p.sh2a = sh2a;
+    p.c2e = c2e;
+    p.t = t;
+    const float itd = frcp(ch2a + c2e), itd2 = itd * itd;
+    p.itd4 = itd2 * itd2;
+    float term = pi05_term32(p, u, v, srem, rem2, h.rc, h.rc2, h.irc);
+    if (TYPE == 81) term -= pi05_term32(p, u, v, srem, rem2, h.rcut, h.rcut2, h.ircut);
+    return h.ppre * term * irem;
 }
 
 /* Kahan compensated accumulation of one FP32 component. */

@@ -36,3 +36,38 @@ def test_rcp_rsqrt_within_few_ulp():
     # reference 1/sqrt(x) in extended precision, rounded once
     ref = (1.0 / np.sqrt(x.astype(np.longdouble))).astype(np.float64)
     assert ulp_diff(rsq, ref).max() <= 2
+
+
+def test_fp32_atan2_and_sqrt():
+    """The FP32 atan2 of the compensated potential (own polynomial) against FP64 atan2 and
+    CUDA's atan2f, and its approximate square root against FP64 sqrt, over the operand
+    range of the pair loops (|x|, |y| in [1e-6, 1e3], every quadrant and the axes)."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lenstool_hpc_b200 import build
+    build.build()
+    L = lt.load_library()
+    fp = C.POINTER(C.c_float)
+    L.lt_eval_fast_math32.argtypes = [C.c_int, C.c_int, fp, fp, fp, fp, fp]
+    rng = np.random.default_rng(2)
+    n = 400000
+    y = (rng.standard_normal(n) * 10.0 ** rng.uniform(-6, 3, n)).astype(np.float32)
+    x = (rng.standard_normal(n) * 10.0 ** rng.uniform(-6, 3, n)).astype(np.float32)
+    y[:4] = [0., -0., 1., -1.]
+    x[:4] = [1., -1., 0., 0.]
+    own, cuda, sq = (np.empty(n, np.float32) for _ in range(3))
+    ptr = lambda a: a.ctypes.data_as(fp)  # noqa: E731
+    assert L.lt_eval_fast_math32(0, n, ptr(y), ptr(x), ptr(own), ptr(cuda), ptr(sq)) == 0
+    ref = np.arctan2(y.astype(np.float64), x.astype(np.float64))
+    err = np.abs(own.astype(np.float64) - ref)
+    assert err.max() <= 4e-7
+    assert np.max(err / np.maximum(np.abs(ref), 1e-30)) <= 4e-7
+    assert np.max(np.abs(own.astype(np.float64) - cuda.astype(np.float64))) <= 6e-7
+    ax = np.abs(x)
+    big = ax > 1e-30
+    rs = np.sqrt(ax[big].astype(np.float64))
+    # sqrt of |x| (the loops take roots of non-negative operands only)
+    sq2 = np.empty(n, np.float32)
+    assert L.lt_eval_fast_math32(0, n, ptr(y), ptr(ax.astype(np.float32)), ptr(own), ptr(cuda), ptr(sq2)) == 0
+    assert np.max(np.abs(sq2[big].astype(np.float64) - rs) / rs) <= 2.4e-7
