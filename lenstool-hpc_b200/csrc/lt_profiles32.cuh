@@ -197,8 +197,8 @@ __device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
     if (TYPE == 8) {
         const float nci = h.s2 * wc - v * h.icx1;
         /* z = N/D: log|z| = (log|N|^2 - log|D|^2)/2, arg z = arg(N conj(D)) */
-        const float lr = 0.5f * (logf(nr * nr + nci * nci) - logf(u * u + dci * dci));
-        const float li = atan2f(nci * u - nr * dci, nr * u + nci * dci);
+        const float lr = 0.5f * __logf((nr * nr + nci * nci) * frcp(u * u + dci * dci));
+        const float li = fatan2(nci * u - nr * dci, nr * u + nci * dci);
         return {h.ppre * li, -h.ppre * lr};
     }
     const float xt = h.rcut2 + rho2;
@@ -216,7 +216,7 @@ __device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
     const float er = (numr * denr + numi * deni) * inv;
     const float ei = (numi * denr - numr * deni) * inv;
     const float lr = 0.5f * log1pf(er * (2.f + er) + ei * ei);
-    const float li = atan2f(ei, 1.f + er);
+    const float li = fatan2(ei, 1.f + er);
     return {h.ppre * li, -h.ppre * lr};
 }
 
