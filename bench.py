@@ -507,13 +507,10 @@ def main():
         return 0
 
     import torch
-    import torch.distributed as dist
     lt = _package()
-    from lenstool_hpc_b200 import build, catalog
+    from lenstool_hpc_b200 import build, catalog, replicas
     torch.cuda.set_device(local_rank)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    replicas.init("nccl", timeout_s=120.0)
     build.build()
     if args.only_batch:
         ctx = lt.Context(local_rank)
@@ -544,9 +541,7 @@ def main():
     ctx.synchronize(stream)
 
     def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
+        replicas.barrier(torch.cuda.synchronize)
 
     props = torch.cuda.get_device_properties(local_rank)
     gpu_id = f"GPU-{props.uuid}" if getattr(props, "uuid", None) else str(local_rank)
@@ -568,11 +563,8 @@ def main():
     launches = lt.launch_count() - n0
     elapsed = t_all0.elapsed_time(t_all1) / 1e3
     per_launch = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)])) / 1e3
-    tmax = torch.tensor([elapsed], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-    elapsed = float(tmax.item())
     evals_step = sums_per_pair * g.npix * cat.n
+    value, elapsed, _ = replicas.throughput(evals_step * args.steps, elapsed, "cuda")
 
     breakdown = None
     if args.breakdown and rank == 0:
@@ -589,7 +581,6 @@ def main():
             ctx.synchronize(stream)
             dt = e0.elapsed_time(e1) / 1e3 / args.steps
             breakdown[label] = {"ms": dt * 1e3, "evals_per_s": g.npix * cat.n / dt}
-    value = world * evals_step * args.steps / elapsed
 
     # the same workload in LT_FP64 (the reference's FP64 arithmetic; Hessian bit-identical)
     fp64_cmp = None
@@ -625,12 +616,10 @@ def main():
             ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp, which=names)
             c2.release()
         torch.cuda.synchronize()
-        te = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_value, _, _ = replicas.throughput(evals_step * args.steps, time.perf_counter() - t0, "cuda")
         h2d = 192 * cat.n + 16 * cat.n
         d2h = len(names) * g.npix * 8
-        e2e = {"value": world * evals_step * args.steps / float(te.item()), "unit": "evals/s",
+        e2e = {"value": e2e_value, "unit": "evals/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "note": "host SoA -> lt_catalog_upload (packed records + chunk table) and 5 float64 maps -> pinned host"}
 
@@ -689,8 +678,7 @@ def main():
             line["chi2_batch"] = bench_chi2(ctx, cpu=not args.no_cpu_baseline)
         print(json.dumps(line))
     ctx.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finalize()
     return 0
 
 
