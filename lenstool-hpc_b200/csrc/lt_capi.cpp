@@ -428,8 +428,9 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
             count_launch(1);
         }
     } else if (precision == LT_FP64) {
-        /* the Hessian with the reference's rounding sequence */
-        const int xop = (op & OP_HESS) ? ((op & ~OP_HESS) | OP_HEX) : op;
+        /* the Hessian with the reference's rounding sequence, the potential through its
+         * pi05 formula */
+        const int xop = ((op & OP_HESS) ? ((op & ~OP_HESS) | OP_HEX) : op) | ((op & OP_POT) ? OP_PEX : 0);
         err = launch_grid64_tiled(xop, a, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
     } else if (precision == LT_FP64_FAST) {
         err = launch_grid64_tiled(op, a, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][op & 7]);

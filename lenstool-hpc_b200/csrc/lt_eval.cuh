@@ -40,7 +40,8 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
                 acc.hxy[k] = hh.xy;
             }
             if (OP & OP_HEX) ex::hess_pair<TYPE>(r, px[k], py, acc.run[k]);
-            if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
+            if ((OP & OP_POT) && (OP & OP_PEX)) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
+            if ((OP & OP_POT) && !(OP & OP_PEX)) pot_pair_fast<TYPE>(r, px[k], py, acc.psi[k]);
         }
     }
 }
@@ -105,7 +106,7 @@ __device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, co
                 acc.hyy[k] = hh.yy;
                 acc.hxy[k] = hh.xy;
             }
-            if (OP & OP_POT) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
+            if (OP & OP_POT) pot_pair_fast<TYPE>(r, px[k], py, acc.psi[k]);
             if (OP & OP_GRAD) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
         }
     }
@@ -134,7 +135,7 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
             if (r.rnear2 == kProxy64) { /* an FP64 proxy record: every term in FP64 */
                 const lt_rec64 &r64 = recs64[r.idx64];
 #pragma unroll
-                for (int k = 0; k < P; k++) pot_pair<TYPE>(r64, px[k], py, acc.psi[k]);
+                for (int k = 0; k < P; k++) pot_pair_fast<TYPE>(r64, px[k], py, acc.psi[k]);
             } else {
 #pragma unroll
                 for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));

@@ -191,7 +191,8 @@ int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool 
     case OP_POT: return launch_shape<OP_POT>(shape, args, num_sms, s);
     case OP_HESS | OP_POT: return launch_shape<OP_HESS | OP_POT>(shape, args, num_sms, s);
     case OP_HEX: return launch_shape<OP_HEX>(shape, args, num_sms, s);
-    case OP_HEX | OP_POT: return launch_shape<OP_HEX | OP_POT>(shape, args, num_sms, s);
+    case OP_POT | OP_PEX: return launch_shape<OP_POT | OP_PEX>(shape, args, num_sms, s);
+    case OP_HEX | OP_POT | OP_PEX: return launch_shape<OP_HEX | OP_POT | OP_PEX>(shape, args, num_sms, s);
     default: return (int)cudaErrorInvalidValue;
     }
 }

@@ -254,6 +254,72 @@ __device__ __forceinline__ void pot_pair(const lt_rec64 &h, double px, double py
     psi += h.pref_h * t / srem;
 }
 
+/* The potential in the cancellation-free form derived in lt_profiles32.cuh (pi05 through
+ * N+- = (cosh 2a + cos 2 eta_im)(1 +- tanh eta tanh zeta), no complex quotient, no branch
+ * wrap), in FP64: per dPIE pair 4 log and 4 atan2 in place of the formula's 16 exp, 6 log,
+ * 4 atan2, asinh, asin and 2 sincos.  Against an extended-precision evaluation of pi05 it
+ * is within 1e-13 of a term's scale where the reference formula in FP64 is within 2e-13
+ * (checked per term over e in [1e-5, 0.73], r in [0.05, 800]). */
+struct Pi05Shared64 {
+    double sh2r, sh2i, E2, iE2, sh2a, c2e, t, itd4;
+};
+
+__device__ __forceinline__ double pi05_term64(const Pi05Shared64 &p, double u, double v, double srem, double rem2,
+                                              double r, double r2)
+{
+    const double q = sqrt(r2 + rem2);
+    const double qr = q + r;
+    const double dm = (srem * qr + rem2) * rcp64(r * qr); /* rho - 1 */
+    const double rho = 1. + dm, rho1 = rho + 1.;
+    const double inv = rcp64(rho * rho1);
+    const double irho = rho1 * inv, irho1 = rho * inv;
+    const double tz = dm * irho1;
+    const double sh2z = 0.5 * dm * rho1 * irho;
+    const double ch2z = 0.25 * rho1 * rho1 * irho;
+    const double m = 2. * irho1 * p.sh2a;
+    const double A = (p.E2 - m) + p.c2e, C = (p.iE2 + m) + p.c2e, B = tz * p.t, B2 = B * B;
+    const double np2 = A * A + B2, nm2 = C * C + B2;
+    const double a2r = 0.5 * log(np2 * rcp64(nm2));
+    const double a2i = atan2(B * (A + C), A * C - B2);
+    const double a1r = -0.5 * log((ch2z * ch2z) * (np2 * nm2) * p.itd4);
+    const double a1i = atan2(2. * B * tz * p.sh2a, A * C + B2);
+    const double kr = (p.sh2r * a1r - p.sh2i * a1i) + sh2z * a2r;
+    const double ki = (p.sh2i * a1r + p.sh2r * a1i) + sh2z * a2i;
+    return r * (ki * u - kr * v);
+}
+
+template <int TYPE>
+__device__ __forceinline__ void pot_pair_fast(const lt_rec64 &h, double px, double py, double &psi)
+{
+    Frame64 f = to_frame(h, px, py);
+    const double u = f.u, v = f.v;
+    const double uu = u * u, vv = v * v;
+    if (TYPE == 5) {
+        psi += h.b0 * sqrt(uu * h.cx1 + vv * h.cx1inv);
+        return;
+    }
+    const double rem2 = uu * h.cxro_inv + vv * h.cyro_inv;
+    const double irem = rsqrt64(rem2), srem = rem2 * irem;
+    const double iz = rsqrt64(uu + vv);
+    const double s = h.e1 * v * iz, t = h.e2 * u * iz;
+    const double g = fabs(s) + sqrt(s * s + 1.);
+    const double ig = rcp64(g);
+    Pi05Shared64 p;
+    p.E2 = s >= 0. ? ig : g;
+    p.iE2 = s >= 0. ? g : ig;
+    const double ch2a = 0.5 * (p.E2 + p.iE2);
+    p.sh2a = 0.5 * (p.E2 - p.iE2);
+    p.c2e = sqrt(fmax(1. - t * t, 0.));
+    p.t = t;
+    p.sh2r = p.sh2a * p.c2e;
+    p.sh2i = ch2a * t;
+    const double itd = rcp64(ch2a + p.c2e), itd2 = itd * itd;
+    p.itd4 = itd2 * itd2;
+    double term = pi05_term64(p, u, v, srem, rem2, h.rc, h.rc2);
+    if (TYPE == 81) term -= pi05_term64(p, u, v, srem, rem2, h.rcut, h.rcut2);
+    psi += h.pref_h * term * irem;
+}
+
 } // namespace lt
 
 /* ------------------------------------------------ reference-exact Hessian ---- */

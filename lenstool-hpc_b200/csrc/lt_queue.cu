@@ -413,8 +413,9 @@ __global__ void __launch_bounds__(kQThreads, 2) queue_kernel(const QArgs q)
         } else {
             if (item.op & OP_GRAD) ok = tile64<OP_GRAD, 1>(item, tile, st, q.status);
             if (ok && hp == OP_HESS) ok = tile64<OP_HEX, 1>(item, tile, st, q.status);
-            if (ok && hp == OP_POT) ok = tile64<OP_POT, 1>(item, tile, st, q.status);
-            if (ok && hp == (OP_HESS | OP_POT)) ok = tile64<OP_HEX | OP_POT, 1>(item, tile, st, q.status);
+            if (ok && hp == OP_POT) ok = tile64<OP_POT | OP_PEX, 1>(item, tile, st, q.status);
+            if (ok && hp == (OP_HESS | OP_POT))
+                ok = tile64<OP_HEX | OP_POT | OP_PEX, 1>(item, tile, st, q.status);
         }
         __syncthreads();
         if (!ok) break; /* a bounded wait gave up; the status word says so */

@@ -84,7 +84,10 @@ def test_grid_vs_oracle(ctx, oracle_lib, cluster_type, shape):
     for k, name in enumerate(["hess_a", "hess_b", "hess_c"]):
         assert max_rel_err(hf[name], oh[k]) <= TOL, name
     psi = ctx.potential_grid(cat, g)
-    assert max_rel_err(psi, oracle_lib.pot_grid(cat, g)) <= TOL
+    opsi = oracle_lib.pot_grid(cat, g)
+    assert max_rel_err(psi, opsi) <= TOL
+    # LT_FP64_FAST takes the potential through the N+- form (as accurate per term)
+    assert max_rel_err(ctx.potential_grid(cat, g, precision="fp64fast"), opsi) <= TOL
 
 
 def test_every_map_kind_vs_oracle(ctx, oracle_lib):
