@@ -49,7 +49,7 @@ FLOPS_PER_PAIR = 182 + 760
 # DRAM bytes (read + write) of one launch of the default step's dominant kernel
 # (grid32c_kernel<OP_HESS|OP_POT>, FP32C, 4096^2 x 1000 halos), from a single-pass ncu
 # capture of this bench's own launch: profiles/launches_lens_maps_fp32c_1000h_4096.md
-TRAFFIC_FP32C_LENS_4096 = 22892800 + 638461440
+TRAFFIC_FP32C_LENS_4096 = 28883968 + 638935808
 
 
 def _package():
