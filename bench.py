@@ -443,6 +443,15 @@ def bench_chi2(ctx, n_models=64, n=2048, nsys=40, seed=20261203 + 3, cpu=True):
            "models_per_s": n_models / dt, "ms_per_model": 1e3 * dt / n_models,
            "seconds_for_4096_models": 4096 * dt / n_models, "deflection_evals_per_s": n_models * n * n * base.n / dt,
            "chi2_true_model": true_chi, "chi2_median_perturbed": float(np.median(chi))}
+    # the deflection grid in LT_FP32C, delensing and chi2 in FP64
+    ctx.chi2(models[:2], frame, n, systems, precision="fp32c")
+    t0 = time.perf_counter()
+    chi32, found32 = ctx.chi2(models, frame, n, systems, precision="fp32c")
+    dt32 = time.perf_counter() - t0
+    res["fp32c_deflections"] = {
+        "models_per_s": n_models / dt32, "ms_per_model": 1e3 * dt32 / n_models,
+        "same_images_found": bool(np.array_equal(found32, found)),
+        "max_rel_chi2_diff": float(np.max(np.abs(chi32 - chi) / np.maximum(np.abs(chi), 1.)))}
     if cpu:
         try:
             import oracle

@@ -380,6 +380,13 @@ lt_status lt_chi2(lt_context *ctx, const lt_catalog *cat, const lt_frame *frame,
 /* chi2 of `nmodels` models against the same systems (chi2[m], images_found[m]). */
 lt_status lt_chi2_batch(lt_context *ctx, const lt_catalog *const *cats, int32_t nmodels, const lt_frame *frame,
                         int32_t n, const lt_image_systems *systems, double *chi2, int32_t *images_found);
+/* lt_chi2_batch with the deflection grid in `precision`: LT_FP64 (as lt_chi2_batch;
+ * LT_FP64_FAST is the same grid) or LT_FP32C, whose grid is within 1e-6 of the FP64 one;
+ * the sources, the delensing and the chi2 reduction are FP64 in every case.  The
+ * reference computes the grid in FP64 (src/chi_CPU_barycenter.cpp:127-137). */
+lt_status lt_chi2_batch_precision(lt_context *ctx, const lt_catalog *const *cats, int32_t nmodels,
+                                  const lt_frame *frame, int32_t n, const lt_image_systems *systems,
+                                  int32_t precision, double *chi2, int32_t *images_found);
 /* Write a host map (nx * ny float64, row j at image row j + 1) as a FITS primary image in
  * the reference's layout (module_writeFits_Image, src/module_writeFits.cpp:113-206):
  * float32 data, BZERO/BSCALE, a linear arcsec WCS with pixel 1 at (xmin, ymin) and

@@ -183,6 +183,8 @@ def load_library(path=None):
     L.lt_chi2.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems), _dp, _ip]
     L.lt_chi2_batch.argtypes = [vp, C.POINTER(vp), C.c_int32, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems), _dp,
                                 _ip]
+    L.lt_chi2_batch_precision.argtypes = [vp, C.POINTER(vp), C.c_int32, C.POINTER(_Frame), C.c_int32,
+                                          C.POINTER(_Systems), C.c_int32, _dp, _ip]
     L.lt_delense.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.c_int32, _dp, _dp, _dp, _ip, _dp, _dp]
     L.lt_kernel_launch_count.restype = C.c_uint64
     L.lt_status_string.restype = C.c_char_p
@@ -400,9 +402,10 @@ class Context:
 
     # ---- strong-lensing chi2 (frame = (xmin, xmax, ymin, ymax) of an n x n grid) ----
 
-    def chi2(self, cats, frame, n, systems):
-        """lt_chi2_batch: chi2 of each catalogue (model) against `systems` (an
-        images.ImageSystems).  Returns (chi2 array, predicted-image counts)."""
+    def chi2(self, cats, frame, n, systems, precision="fp64"):
+        """lt_chi2_batch_precision: chi2 of each catalogue (model) against `systems` (an
+        images.ImageSystems), the deflection grid in `precision` ("fp64" or "fp32c"; the
+        delensing and the chi2 are FP64).  Returns (chi2 array, predicted-image counts)."""
         single = not isinstance(cats, (list, tuple))
         cl = [self._cat(c) for c in ([cats] if single else cats)]
         s = systems.contiguous()
@@ -411,9 +414,10 @@ class Context:
         handles = (C.c_void_p * len(cl))(*[c.handle.value if hasattr(c.handle, "value") else c.handle for c in cl])
         chi = np.empty(len(cl))
         found = np.empty(len(cl), np.int32)
-        st = self._lib.lt_chi2_batch(self.handle, handles, len(cl), C.byref(_Frame(*frame)), n, C.byref(sy),
-                                     chi.ctypes.data_as(_dp), found.ctypes.data_as(_ip))
-        self._check(st, "lt_chi2_batch")
+        st = self._lib.lt_chi2_batch_precision(self.handle, handles, len(cl), C.byref(_Frame(*frame)), n,
+                                               C.byref(sy), PRECISION[precision], chi.ctypes.data_as(_dp),
+                                               found.ctypes.data_as(_ip))
+        self._check(st, "lt_chi2_batch_precision")
         return (chi[0], int(found[0])) if single else (chi, found)
 
     def delense(self, cat, frame, n, bx, by, dlsds):

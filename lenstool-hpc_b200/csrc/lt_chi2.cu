@@ -390,8 +390,11 @@ lt_status check_systems(lt_context *ctx, const lt_image_systems *sys)
     return LT_OK;
 }
 
-/* Steps 1-4 for one catalogue on the prepared buffers (stream-ordered). */
-int chi2_launch(lt_context *ctx, const lt_catalog *cat, Chi2Buf &b, bool sources_given, bool link, cudaStream_t s)
+/* Steps 1-4 for one catalogue on the prepared buffers (stream-ordered).  The deflection
+ * grid of step 1 is FP64, or FP32C with precision LT_FP32C; the sources, the delensing and
+ * the chi2 are FP64 either way. */
+int chi2_launch(lt_context *ctx, const lt_catalog *cat, Chi2Buf &b, bool sources_given, bool link, cudaStream_t s,
+                int precision = LT_FP64)
 {
     Chi2Dev &c = b.dev;
     GridArgs a;
@@ -419,6 +422,8 @@ int chi2_launch(lt_context *ctx, const lt_catalog *cat, Chi2Buf &b, bool sources
     if (cat->nhalos == 0) {
         err = (int)cudaMemsetAsync((void *)c.ax, 0, 8 * (size_t)c.n * c.n, s);
         if (err == cudaSuccess) err = (int)cudaMemsetAsync((void *)c.ay, 0, 8 * (size_t)c.n * c.n, s);
+    } else if (precision == LT_FP32C) {
+        err = launch_fp32c(ctx, cat, OP_GRAD, a, s);
     } else {
         err = launch_grid64_tiled(OP_GRAD, a, ctx->num_sms, s, ctx->shape[LT_FP64][OP_GRAD]);
     }
@@ -490,11 +495,16 @@ lt_status lt_delense(lt_context *ctx, const lt_catalog *cat, const lt_frame *fra
     return LT_OK;
 }
 
-lt_status lt_chi2_batch(lt_context *ctx, const lt_catalog *const *cats, int32_t nmodels, const lt_frame *frame,
-                        int32_t n, const lt_image_systems *sys, double *chi2, int32_t *images_found)
+lt_status lt_chi2_batch_precision(lt_context *ctx, const lt_catalog *const *cats, int32_t nmodels,
+                                  const lt_frame *frame, int32_t n, const lt_image_systems *sys, int32_t precision,
+                                  double *chi2, int32_t *images_found)
 {
     if (!ctx || !cats || nmodels < 1 || !frame_ok(frame, n) || !chi2) {
         if (ctx) set_error(ctx, "invalid chi2 arguments");
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    if (precision != LT_FP64 && precision != LT_FP64_FAST && precision != LT_FP32C) {
+        set_error(ctx, "chi2: unknown precision %d", precision);
         return LT_ERR_INVALID_ARGUMENT;
     }
     for (int m = 0; m < nmodels; m++)
@@ -522,7 +532,7 @@ lt_status lt_chi2_batch(lt_context *ctx, const lt_catalog *const *cats, int32_t 
     if (st == LT_OK) st = dev_alloc(ctx, (void **)&d_res, 16 * (size_t)nmodels);
     int err = cudaSuccess;
     for (int m = 0; st == LT_OK && m < nmodels && err == cudaSuccess; m++) {
-        err = chi2_launch(ctx, cats[m], b, false, true, s);
+        err = chi2_launch(ctx, cats[m], b, false, true, s, precision);
         if (err == cudaSuccess) err = (int)cudaMemcpyAsync(d_res + 2 * m, b.dev.chi2, 8, cudaMemcpyDeviceToDevice, s);
         if (err == cudaSuccess)
             err = (int)cudaMemcpyAsync(d_res + 2 * m + 1, b.dev.found, 8, cudaMemcpyDeviceToDevice, s);
@@ -550,6 +560,12 @@ lt_status lt_chi2_batch(lt_context *ctx, const lt_catalog *const *cats, int32_t 
         return LT_ERR_QUEUE_FULL;
     }
     return LT_OK;
+}
+
+lt_status lt_chi2_batch(lt_context *ctx, const lt_catalog *const *cats, int32_t nmodels, const lt_frame *frame,
+                        int32_t n, const lt_image_systems *sys, double *chi2, int32_t *images_found)
+{
+    return lt_chi2_batch_precision(ctx, cats, nmodels, frame, n, sys, LT_FP64, chi2, images_found);
 }
 
 lt_status lt_chi2(lt_context *ctx, const lt_catalog *cat, const lt_frame *frame, int32_t n,

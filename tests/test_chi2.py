@@ -86,3 +86,22 @@ def test_chi2_rejects_bad_systems(ctx, setup):
     assert e.value.status == 1
     with pytest.raises(lt.LensError):
         ctx.chi2(dcat, (0., -1., 0., 1.), 64, s)
+
+
+def test_chi2_fp32c_deflections(ctx, setup):
+    """The deflection grid in LT_FP32C (within 1e-6 of the FP64 grid), the sources,
+    delensing and chi2 in FP64.  A predicted image is the image-plane barycentre of a grid
+    triangle whose source-plane image contains the source (src/delense_CPU.cpp:117-118), so
+    the grid's deflections enter only through the inclusion tests: chi2 changes only where
+    a source lies within ~1e-5" of a source-plane triangle's edge, which none of these
+    models' sources does (the same images, chi2 equal well inside 1e-3)."""
+    cat, dcat, s = setup
+    rng = np.random.Generator(np.random.PCG64(9))
+    handles = [dcat] + [ctx.upload(catalog.perturb_catalog(cat, rng)) for _ in range(7)]
+    for n in (512, 1024):
+        c64, f64 = ctx.chi2(handles, FRAME, n, s)
+        c32, f32 = ctx.chi2(handles, FRAME, n, s, precision="fp32c")
+        rel = np.abs(c32 - c64) / np.maximum(np.abs(c64), 1.)
+        print(n, "found", f64.tolist(), f32.tolist(), "max rel chi2 diff", rel.max())
+        assert np.array_equal(f32, f64)
+        assert rel.max() <= 1e-3
