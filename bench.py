@@ -332,15 +332,18 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
     return res
 
 
-def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=8, seed=20261203 + 4):
+def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=12, seed=20261203 + 4):
     """Serving workload: Poisson arrivals at `rate` req/s of requests drawn uniformly from
-    {deflection map, kappa/gamma1/gamma2/mu maps}, grids U{512^2, 1024^2, 2048^2, 4096^2},
-    catalogues with log-uniform(50, 5000) halos (1% cluster-scale) resident in HBM.  The
-    serving loop's p50/p99 latency (submission to results in HBM) and maps/s, against the
-    same requests as one plain FP64 call each."""
+    {deflection map, kappa/gamma1/gamma2/mu maps, chi2}, grids U{512^2, 1024^2, 2048^2,
+    4096^2}.  Map requests use catalogues with log-uniform(50, 5000) halos (1% cluster-scale)
+    resident in HBM; chi2 requests one of 8 perturbed models of the 200-halo catalogue
+    against 40 image systems (as the chi2 workload).  The serving loop's p50/p99 latency
+    (submission to results in HBM) and throughput, against the same requests as one plain
+    FP64 call each."""
     import torch
     lt = _package()
     from lenstool_hpc_b200 import catalog
+    from lenstool_hpc_b200.images import generate_systems
     rng = np.random.Generator(np.random.PCG64(seed))
     pool = []
     for i in range(12):
@@ -348,23 +351,32 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=8, see
         nc = max(1, int(round(0.01 * n)))
         pool.append(catalog.cluster_galaxy_catalog(nc, n - nc, seed + 100 + i))
     dcats = [ctx.upload(c) for c in pool]
-    kinds_of = (("deflection_x", "deflection_y"), ("kappa", "gamma1", "gamma2", "mu"))
+    frame = (-100., 100., -100., 100.)
+    base = catalog.cluster_galaxy_catalog(2, 198, 20261203)
+    dbase = ctx.upload(base)
+    ic = int(np.argmax(base.b0))
+    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
+    D = dls / dos
+    systems = generate_systems(lambda bx, by, dr: ctx.delense(dbase, frame, 2048, bx, by, dr), 40, 20261203 + 3,
+                               dr=D, centre=(base.position_x[ic], base.position_y[ic]), source_radius=10.)
+    models = [ctx.upload(catalog.perturb_catalog(base, rng)) for _ in range(8)]
+    kinds_of = (("deflection_x", "deflection_y"), ("kappa", "gamma1", "gamma2", "mu"), ())
     reqs = []
     for i in range(n_requests):
-        k = int(rng.integers(2))
+        k = int(rng.integers(3))
         n = int(rng.choice([512, 1024, 2048, 4096]))
-        c = int(rng.integers(len(pool)))
+        c = int(rng.integers(len(pool) if k < 2 else len(models)))
         reqs.append((k, n, c))
     gaps = rng.exponential(1.0 / rate, n_requests)
     arrivals = np.cumsum(gaps) - gaps[0]
-    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
-    D = dls / dos
     outs = [{kk: torch.empty((n, n), dtype=torch.float64, device="cuda") for kk in kinds_of[k]} for k, n, c in reqs]
-    evals = float(sum(n * n * pool[c].n for k, n, c in reqs))
+    halos = lambda k, c: pool[c].n if k < 2 else base.n  # noqa: E731
+    evals = float(sum(n * n * halos(k, c) for k, n, c in reqs))
     nmaps = sum(len(kinds_of[k]) for k, n, c in reqs)
+    nchi = sum(1 for k, n, c in reqs if k == 2)
 
     def run(arr):
-        with ctx.server(precision=precision, slots=64, window=8) as srv:
+        with ctx.server(precision=precision, slots=64, window=8, output_bytes=8 << 30) as srv:
             # warm-up request (the loop kernel's first launch)
             w = {"kappa": torch.empty((64, 64), dtype=torch.float64, device="cuda")}
             srv.wait(srv.submit(lt.Request(dcats[0], catalog.Grid.square(100., 64), w, dlsds=D)))
@@ -374,25 +386,36 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=8, see
                 now = time.perf_counter() - t0
                 if ta > now:
                     time.sleep(ta - now)
-                tickets.append(srv.submit(lt.Request(dcats[c], catalog.Grid.square(100., n), o, dlsds=D, scale=D)))
+                if k == 2:
+                    tickets.append(srv.submit_chi2(models[c], frame, n, systems))
+                else:
+                    tickets.append(srv.submit(lt.Request(dcats[c], catalog.Grid.square(100., n), o, dlsds=D,
+                                                         scale=D)))
             for t in tickets:
                 srv.wait(t, 3600.)
             t_end = time.perf_counter() - t0
             lat = [srv.times(t)[2] for t in tickets]
+            lat_chi = [x for x, (k, n, c) in zip(lat, reqs) if k == 2]
+            lat_map = [x for x, (k, n, c) in zip(lat, reqs) if k != 2]
             st = srv.stats()
-        return {"p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99), "maps_per_s": nmaps / t_end,
-                "requests_per_s": len(reqs) / t_end, "evals_per_s": evals / t_end, "seconds": t_end,
-                "max_inflight": st["max_inflight"], "loop_launches": st["loop_launches"]}
+        return {"p50_ms": _percentile(lat, 50), "p99_ms": _percentile(lat, 99),
+                "maps": {"p50_ms": _percentile(lat_map, 50), "p99_ms": _percentile(lat_map, 99)},
+                "chi2": {"p50_ms": _percentile(lat_chi, 50), "p99_ms": _percentile(lat_chi, 99)},
+                "requests_per_s": len(reqs) / t_end, "maps_per_s": nmaps / t_end, "chi2_per_s": nchi / t_end,
+                "evals_per_s": evals / t_end, "seconds": t_end, "max_inflight": st["max_inflight"],
+                "loop_launches": st["loop_launches"]}
 
     res = {"workload": f"serving: {n_requests} requests, Poisson {rate:g}/s, grids U{{512..4096}}^2, "
-                       f"halos log-U(50,5000), deflection or kappa/gamma/mu maps (chi2 requests not built)",
+                       f"deflection or kappa/gamma/mu maps (halos log-U(50,5000)) or chi2 (200 halos, "
+                       f"40 systems): {n_requests - nchi} map and {nchi} chi2 requests",
            "precision": precision}
     sat = run(arrivals)
     res["at_rate"] = dict(sat, rate_per_s=rate, offered_over_capacity=rate / sat["requests_per_s"])
     # a second pass at 70% of the measured capacity (the queue does not build up)
     r70 = 0.7 * sat["requests_per_s"]
     res["at_70pct_capacity"] = dict(run(arrivals * rate / r70), rate_per_s=r70)
-    # one plain FP64 call per request (host outputs, the reference's calling pattern)
+    # one plain FP64 call per request (host outputs / host chi2, the reference's calling
+    # pattern), a sample scaled to all requests by halo x pixel evaluations of their grids
     idx = list(range(plain_sample))
     t0 = time.perf_counter()
     for i in idx:
@@ -400,15 +423,18 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=8, see
         g = catalog.Grid.square(100., n)
         if k == 0:
             ctx.gradient_grid(dcats[c], g, precision="fp64", scale=D)
-        else:
+        elif k == 1:
             ctx.hessian_maps(dcats[c], g, list(kinds_of[1]), precision="fp64", dlsds=D)
+        else:
+            ctx.chi2(models[c], frame, n, systems)
     t = time.perf_counter() - t0
-    sample_evals = float(sum(reqs[i][1] ** 2 * pool[reqs[i][2]].n for i in idx))
-    # the sample's time scaled to all requests by halo x pixel evaluations
-    res["one_request_per_call_fp64"] = {"maps_per_s": nmaps / (t * evals / sample_evals),
+    sample_evals = float(sum(reqs[i][1] ** 2 * halos(reqs[i][0], reqs[i][2]) for i in idx))
+    t_all = t * evals / sample_evals
+    res["one_request_per_call_fp64"] = {"requests_per_s": len(reqs) / t_all, "maps_per_s": nmaps / t_all,
                                         "sample_requests": len(idx), "sample_s": t}
-    res["speedup_vs_one_request_per_call_fp64"] = sat["maps_per_s"] / res["one_request_per_call_fp64"]["maps_per_s"]
-    for c in dcats:
+    res["speedup_vs_one_request_per_call_fp64"] = (sat["requests_per_s"] /
+                                                   res["one_request_per_call_fp64"]["requests_per_s"])
+    for c in dcats + models + [dbase]:
         c.release()
     return res
 

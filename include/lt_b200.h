@@ -400,6 +400,19 @@ lt_status lt_delense(lt_context *ctx, const lt_catalog *cat, const lt_frame *fra
                      const double *bx, const double *by, const double *dlsds, int32_t *nfound, double *fx,
                      double *fy);
 
+/* A chi2 request to the serving loop: the chi2 of `cat` against `systems` on an n x n grid
+ * over `frame`, as lt_chi2_batch_precision in the server's precision.  Its deflection grid
+ * is served by the persistent loop tile by tile like a map request (the grid, the systems
+ * and the work buffers take arena bytes until the result is in); the loop then yields the
+ * GPU at its next tile boundary for the delensing and chi2 kernels and resumes the other
+ * requests' remaining tiles.  The systems are copied at submission.  No counterpart in the
+ * reference, whose chi2 is one blocking call per model (src/chi_CPU_barycenter.cpp:58). */
+lt_status lt_server_submit_chi2(lt_server *server, const lt_catalog *cat, const lt_frame *frame, int32_t n,
+                                const lt_image_systems *systems, uint64_t *ticket);
+/* The chi2 and predicted-image count of a completed chi2 ticket (LT_ERR_NOT_READY before;
+ * LT_ERR_QUEUE_FULL, with the values, when a source had more than LT_MAX_IMAGES images). */
+lt_status lt_server_chi2_result(lt_server *server, uint64_t ticket, double *chi2, int32_t *images_found);
+
 /* Wait for the context's work on `stream` and report any status a kernel recorded
  * (e.g. LT_ERR_TIMEOUT from a bounded device-side wait).  Asynchronous (device-pointer)
  * calls report such errors here. */

@@ -132,7 +132,8 @@ EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release",
            "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
            "lt_server_get_stats", "lt_server_destroy", "lt_chi2", "lt_chi2_batch", "lt_delense",
            "lt_catalog_update", "lt_write_fits", "lt_eval_fast_math", "lt_eval_fast_math32", "lt_bayes_create",
-           "lt_bayes_apply", "lt_bayes_destroy")
+           "lt_bayes_apply", "lt_bayes_destroy", "lt_chi2_batch_precision", "lt_server_submit_chi2",
+           "lt_server_chi2_result")
 SUMS = {"deflection": 1, "hessian": 2, "potential": 4, "lens": 6}
 
 
@@ -175,6 +176,9 @@ def load_library(path=None):
     L.lt_server_release.argtypes = [vp, C.c_uint64]
     L.lt_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
     L.lt_server_destroy.argtypes = [vp]
+    L.lt_server_submit_chi2.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems),
+                                        C.POINTER(C.c_uint64)]
+    L.lt_server_chi2_result.argtypes = [vp, C.c_uint64, _dp, _ip]
     L.lt_catalog_update.argtypes = [vp, vp, C.POINTER(_HaloParams), vp]
     L.lt_bayes_create.argtypes = [vp, C.POINTER(_BayesModel), C.c_int32, C.POINTER(_Potfile), C.c_int32, _ip,
                                   C.POINTER(vp)]
@@ -573,6 +577,27 @@ class Server:
         self.ctx._check(st, "lt_server_submit")
         self._keep[t.value] = request
         return t.value
+
+    def submit_chi2(self, cat, frame, n, systems) -> int:
+        """lt_server_submit_chi2: the chi2 of the resident catalogue `cat` against `systems`
+        (images.ImageSystems) on an n x n grid over `frame`; the result comes from
+        chi2_result once the ticket completes."""
+        s = systems.contiguous()
+        sy = _Systems(s.nsys, s.nimg.ctypes.data_as(_ip), s.x.ctypes.data_as(_dp), s.y.ctypes.data_as(_dp),
+                      s.dr.ctypes.data_as(_dp))
+        t = C.c_uint64()
+        st = self._lib.lt_server_submit_chi2(self.handle, cat.handle, C.byref(_Frame(*frame)), n, C.byref(sy),
+                                             C.byref(t))
+        self.ctx._check(st, "lt_server_submit_chi2")
+        self._keep[t.value] = cat
+        return t.value
+
+    def chi2_result(self, ticket: int):
+        """(chi2, predicted images) of a completed chi2 ticket."""
+        chi, found = C.c_double(), C.c_int32()
+        st = self._lib.lt_server_chi2_result(self.handle, ticket, C.byref(chi), C.byref(found))
+        self.ctx._check(st, "lt_server_chi2_result")
+        return chi.value, found.value
 
     def poll(self, ticket: int) -> bool:
         st = self._lib.lt_server_poll(self.handle, ticket)

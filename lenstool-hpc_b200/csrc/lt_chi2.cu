@@ -28,6 +28,7 @@
 
 #include <cuda_runtime.h>
 
+#include "lt_chi2.h"
 #include "lt_eval.cuh"
 #include "lt_internal.h"
 
@@ -35,26 +36,6 @@ namespace lt {
 
 constexpr int kMaxImg = LT_MAX_IMAGES;  /* predicted images kept per source */
 constexpr int kHitCap = 64;             /* delensing hits recorded per source */
-
-struct Chi2Dev {
-    /* systems */
-    int nsys, nimages;
-    const int32_t *nimg, *first;        /* images per system, index of its first image */
-    const double *ix, *iy, *dr;
-    /* grid */
-    int n;
-    double xmin, ymin, dx, dy;
-    const double *ax, *ay;              /* deflection grid, n x n */
-    /* work */
-    double *bx, *by;                    /* source per system */
-    int32_t *hits, *keys;               /* hit count and hit keys (2 * cell + lower) per system */
-    /* results */
-    double *chi_terms;                  /* per observed image: its chi2 term */
-    double *chi2;                       /* [0]: chi2; written by the reduction */
-    int32_t *found;                     /* [0]: predicted images; [1]: 1 if a source overflowed */
-    int32_t *nfound;                    /* predicted images per system (<= kMaxImg) */
-    double *fx, *fy;                    /* predicted images, nsys x kMaxImg */
-};
 
 /* ---- step 2: sources ------------------------------------------------------------- */
 
@@ -306,9 +287,13 @@ struct Chi2Buf {
     Chi2Dev dev;
 };
 
-lt_status chi2_buffers(lt_context *ctx, int nsys, int nimages, const lt_frame *f, int n, Chi2Buf &b)
+} // namespace
+
+namespace lt {
+
+size_t chi2_layout(int nsys, int nimages, const lt_frame *f, int n, char *m, Chi2Dev &c)
 {
-    memset(&b.dev, 0, sizeof(b.dev));
+    memset(&c, 0, sizeof(c));
     const size_t ns = (size_t)nsys, ni = (size_t)(nimages > 0 ? nimages : 1);
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -321,11 +306,7 @@ lt_status chi2_buffers(lt_context *ctx, int nsys, int nimages, const lt_frame *f
                  o_keys = take(4 * ns * kHitCap), o_terms = take(8 * ni), o_chi = take(8), o_found = take(8),
                  o_nf = take(4 * ns), o_fx = take(8 * ns * kMaxImg), o_fy = take(8 * ns * kMaxImg),
                  o_ax = take(8 * (size_t)n * n), o_ay = take(8 * (size_t)n * n);
-    b.bytes = off;
-    lt_status st = dev_alloc(ctx, &b.mem, b.bytes);
-    if (st != LT_OK) return st;
-    char *m = (char *)b.mem;
-    Chi2Dev &c = b.dev;
+    if (!m) return off;
     c.nsys = nsys;
     c.nimages = nimages;
     c.nimg = (const int32_t *)(m + o_nimg);
@@ -350,7 +331,29 @@ lt_status chi2_buffers(lt_context *ctx, int nsys, int nimages, const lt_frame *f
     c.ymin = f->ymin;
     c.dx = (f->xmax - f->xmin) / (n - 1); /* src/chi_CPU_barycenter.cpp:104-105 */
     c.dy = (f->ymax - f->ymin) / (n - 1);
+    return off;
+}
+
+lt_status chi2_buffers(lt_context *ctx, int nsys, int nimages, const lt_frame *f, int n, Chi2Buf &b)
+{
+    b.bytes = chi2_layout(nsys, nimages, f, n, nullptr, b.dev);
+    lt_status st = dev_alloc(ctx, &b.mem, b.bytes);
+    if (st != LT_OK) return st;
+    chi2_layout(nsys, nimages, f, n, (char *)b.mem, b.dev);
     return LT_OK;
+}
+
+cudaError_t chi2_upload_systems_async(const Chi2Dev &c, const int32_t *nimg, const int32_t *first, const double *x,
+                                      const double *y, const double *dr, cudaStream_t s)
+{
+    cudaError_t e = cudaMemcpyAsync((void *)c.nimg, nimg, 4 * (size_t)c.nsys, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((void *)c.first, first, 4 * (size_t)c.nsys, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && c.nimages)
+        e = cudaMemcpyAsync((void *)c.ix, x, 8 * (size_t)c.nimages, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && c.nimages)
+        e = cudaMemcpyAsync((void *)c.iy, y, 8 * (size_t)c.nimages, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((void *)c.dr, dr, 8 * (size_t)c.nsys, cudaMemcpyHostToDevice, s);
+    return e;
 }
 
 lt_status upload_systems(lt_context *ctx, const lt_image_systems *sys, Chi2Buf &b, cudaStream_t s)
@@ -361,16 +364,7 @@ lt_status upload_systems(lt_context *ctx, const lt_image_systems *sys, Chi2Buf &
         first[i] = total;
         total += sys->nimages[i];
     }
-    Chi2Dev &c = b.dev;
-    cudaError_t e = cudaMemcpyAsync((void *)c.nimg, sys->nimages, 4 * (size_t)sys->nsystems, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync((void *)c.first, first.data(), 4 * first.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && total)
-        e = cudaMemcpyAsync((void *)c.ix, sys->x, 8 * (size_t)total, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && total)
-        e = cudaMemcpyAsync((void *)c.iy, sys->y, 8 * (size_t)total, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync((void *)c.dr, sys->dlsds, 8 * (size_t)sys->nsystems, cudaMemcpyHostToDevice, s);
+    cudaError_t e = chi2_upload_systems_async(b.dev, sys->nimages, first.data(), sys->x, sys->y, sys->dlsds, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s); /* `first` is a local vector */
     if (e != cudaSuccess) return cuda_fail(ctx, e, "image systems upload");
     return LT_OK;
@@ -388,6 +382,24 @@ lt_status check_systems(lt_context *ctx, const lt_image_systems *sys)
             return LT_ERR_INVALID_ARGUMENT;
         }
     return LT_OK;
+}
+
+/* Steps 2-4 on a layout whose deflection planes hold the grid (stream-ordered). */
+static int chi2_steps(lt_context *ctx, const lt_catalog *cat, const Chi2Dev &c, bool sources_given, cudaStream_t s)
+{
+    if (!sources_given) {
+        chi2_sources_kernel<<<c.nsys, 64, 0, s>>>(c, cat->recs, cat->chunks, cat->nhalos ? cat->nchunks : 0);
+        count_launch(1);
+    } else {
+        cudaMemsetAsync(c.hits, 0, 4 * (size_t)c.nsys, s);
+    }
+    const size_t smem = 24 * (size_t)c.nsys;
+    chi2_delense_kernel<<<ctx->num_sms * 8, 256, smem, s>>>(c);
+    count_launch(1);
+    cudaMemsetAsync(c.found, 0, 8, s);
+    chi2_link_kernel<<<1, 256, 0, s>>>(c);
+    count_launch(1);
+    return (int)cudaGetLastError();
 }
 
 /* Steps 1-4 for one catalogue on the prepared buffers (stream-ordered).  The deflection
@@ -428,23 +440,16 @@ int chi2_launch(lt_context *ctx, const lt_catalog *cat, Chi2Buf &b, bool sources
         err = launch_grid64_tiled(OP_GRAD, a, ctx->num_sms, s, ctx->shape[LT_FP64][OP_GRAD]);
     }
     if (err != cudaSuccess) return err;
-    if (!sources_given) {
-        chi2_sources_kernel<<<c.nsys, 64, 0, s>>>(c, cat->recs, cat->chunks, cat->nhalos ? cat->nchunks : 0);
-        count_launch(1);
-    } else {
-        cudaMemsetAsync(c.hits, 0, 4 * (size_t)c.nsys, s);
-    }
-    const size_t smem = 24 * (size_t)c.nsys;
-    chi2_delense_kernel<<<ctx->num_sms * 8, 256, smem, s>>>(c);
-    count_launch(1);
-    cudaMemsetAsync(c.found, 0, 8, s);
-    chi2_link_kernel<<<1, 256, 0, s>>>(c);
-    count_launch(1);
     (void)link;
-    return (int)cudaGetLastError();
+    return chi2_steps(ctx, cat, c, sources_given, s);
 }
 
-} // namespace
+int chi2_tail(lt_context *ctx, const lt_catalog *cat, const Chi2Dev &c, cudaStream_t s)
+{
+    return chi2_steps(ctx, cat, c, false, s);
+}
+
+} // namespace lt
 
 extern "C" {
 

@@ -380,11 +380,25 @@ __global__ void __launch_bounds__(kQThreads, 2) queue_kernel(const QArgs q)
     for (;;) {
         if (tid == 0) {
             int slot = -1, tile = 0;
+            bool counted = false; /* this CTA is in QState::idle */
             for (int polls = 0;; polls++) {
-                if (claim_tile(q, slot, tile)) break;
+                if (*(volatile int32_t *)&q.state->yield) break;
+                if (claim_tile(q, slot, tile)) {
+                    if (counted) atomicSub(&q.state->idle, 1);
+                    break;
+                }
                 slot = -1;
                 if (*(volatile int32_t *)&q.state->stop) break;
-                if (polls >= q.idle_polls) break;
+                if (!counted) {
+                    atomicAdd(&q.state->idle, 1);
+                    counted = true;
+                }
+                /* leave on idle only together: a CTA that left alone would leave work that
+                 * arrives later to fewer CTAs until the whole launch ends */
+                if (polls >= q.idle_polls && *(volatile int32_t *)&q.state->idle >= (int32_t)gridDim.x) {
+                    atomicExch(&q.state->yield, 1);
+                    break;
+                }
                 __nanosleep(1000);
             }
             s_slot = slot;
@@ -443,6 +457,8 @@ __global__ void queue_reset_kernel(QSlot *slots, QState *state, int n)
         state->head = 0ull;
         state->rotor = 0ull;
         state->stop = 1;
+        state->yield = 0;
+        state->idle = 0;
     }
 }
 

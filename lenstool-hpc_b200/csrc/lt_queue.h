@@ -48,6 +48,8 @@ struct alignas(16) QState {
     unsigned long long head;       /* oldest request that may have unclaimed tiles */
     unsigned long long rotor;      /* round-robin counter over the window */
     int32_t stop;                  /* leave when no published request has work */
+    int32_t yield;                 /* leave at the next claim; unclaimed tiles stay for the next launch */
+    int32_t idle;                  /* CTAs of the running launch without work (or gone) */
     int32_t pad;
 };
 

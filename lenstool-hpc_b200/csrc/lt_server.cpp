@@ -20,6 +20,7 @@
  * frees its buffers (src/grid_map_ampli_GPU.cu:93-192).
  */
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -35,6 +36,7 @@
 
 #include "../../include/lt_b200.h"
 #include "lt_arena.h"
+#include "lt_chi2.h"
 #include "lt_internal.h"
 #include "lt_queue.h"
 
@@ -82,12 +84,15 @@ void destroy_extensions(lt_context *ctx)
 
 namespace {
 
-enum { R_QUEUED = 0, R_RUNNING = 1, R_COPYING = 2, R_DONE = 3, R_FAILED = 4 };
+/* R_TAIL: a chi2 request whose deflection grid is done, waiting for its delensing */
+enum { R_QUEUED = 0, R_RUNNING = 1, R_COPYING = 2, R_DONE = 3, R_FAILED = 4, R_TAIL = 5 };
+enum { K_MAPS = 0, K_CHI2 = 1 };
 
 using Clock = std::chrono::steady_clock;
 
 struct SrvReq {
     uint64_t ticket = 0;
+    int kind = K_MAPS;
     lt_request req;
     bool host_out = false;
     size_t plane = 0;          /* bytes per output plane */
@@ -98,6 +103,16 @@ struct SrvReq {
     lt_status status = LT_OK;
     Clock::time_point t_submit, t_admit, t_gpu, t_done;
     cudaEvent_t copied = nullptr;
+    /* chi2 requests: the systems (host copies), the device layout in the arena, results */
+    lt_frame frame{};
+    int n = 0;
+    std::vector<int32_t> nimg, first;
+    std::vector<double> ix, iy, dr;
+    size_t chi_bytes = 0;
+    Chi2Dev dev{};
+    double chi2 = 0.;
+    int32_t found = 0;
+    bool overflow = false;
 };
 
 double ms_between(Clock::time_point a, Clock::time_point b)
@@ -121,9 +136,12 @@ struct lt_server {
     uint32_t *h_flags = nullptr;         /* mapped completion words */
     uint32_t *d_flags = nullptr;
     int32_t *h_status = nullptr;         /* pinned copy of the device status word */
+    double *h_chi = nullptr;             /* pinned chi2 results, two words per slot */
+    int32_t *h_yield = nullptr;          /* pinned {1, 0}: the values written to QState::yield */
     cudaStream_t loop_stream = nullptr, pub_stream = nullptr, copy_stream = nullptr;
     cudaEvent_t loop_done = nullptr;
     bool loop_launched = false;
+    bool yielding = false;               /* QState::yield was set and not yet cleared */
     std::thread thr;
     std::mutex mu;
     std::condition_variable cv_done, cv_work;
@@ -167,7 +185,26 @@ void admit(lt_server *s)
         const int slot = (int)(s->next_seq % (uint64_t)s->nslots);
         if (s->ring[slot]) return; /* the slot's previous request is still running */
         double *outs[LT_MAX_MAPS] = {};
-        if (r->host_out) {
+        if (r->kind == K_CHI2) {
+            /* the chi2 buffers and the deflection planes in the arena; the systems are
+             * copied on the publish stream ahead of the grid's descriptor */
+            const size_t off = s->arena.alloc(r->chi_bytes);
+            if (off == Arena::kFail) return;
+            r->arena_off = off;
+            chi2_layout((int)r->nimg.size(), (int)r->ix.size(), &r->frame, r->n, s->arena_mem + off, r->dev);
+            const cudaError_t e = chi2_upload_systems_async(r->dev, r->nimg.data(), r->first.data(), r->ix.data(),
+                                                            r->iy.data(), r->dr.data(), s->pub_stream);
+            if (e != cudaSuccess) {
+                s->pending.pop_front();
+                set_error(s->ctx, "chi2 systems upload: %s", cudaGetErrorString(e));
+                finish(s, r, LT_ERR_CUDA);
+                s->cv_done.notify_all();
+                continue;
+            }
+            r->req.grid = {r->dev.xmin, r->dev.ymin, r->dev.dx, r->dev.dy, r->n, r->n, 0, 0};
+            outs[0] = (double *)r->dev.ax;
+            outs[1] = (double *)r->dev.ay;
+        } else if (r->host_out) {
             const size_t off = s->arena.alloc(r->plane * (size_t)r->req.nmaps);
             if (off == Arena::kFail) return; /* waits for results to free arena space */
             r->arena_off = off;
@@ -217,6 +254,10 @@ bool collect(lt_server *s)
             if (f != (uint32_t)r->seq + 1u) continue;
             r->t_gpu = Clock::now();
             any = true;
+            if (r->kind == K_CHI2) { /* the grid is done: delensing next (run_tails) */
+                r->state = R_TAIL;
+                continue;
+            }
             if (!r->host_out) {
                 finish(s, r, LT_OK);
                 continue;
@@ -239,10 +280,66 @@ bool collect(lt_server *s)
             const cudaError_t e = cudaEventQuery(r->copied);
             if (e == cudaErrorNotReady) continue;
             any = true;
+            if (e == cudaSuccess && r->kind == K_CHI2) {
+                r->chi2 = s->h_chi[2 * slot];
+                int32_t f[2];
+                memcpy(f, &s->h_chi[2 * slot + 1], sizeof(f));
+                r->found = f[0];
+                r->overflow = f[1] != 0;
+            }
             finish(s, r, e == cudaSuccess ? LT_OK : LT_ERR_CUDA);
         }
     }
     return any;
+}
+
+/* Delensing and chi2 of the chi2 requests whose grids are done.  They run on the loop
+ * stream between two launches of the persistent kernel, which otherwise holds every SM:
+ * the kernel is asked to leave at its next claim (QState::yield; unclaimed tiles stay in
+ * their slots), the tails run with the whole GPU, and the loop is relaunched after them. */
+void run_tails(lt_server *s)
+{
+    bool waiting = false;
+    for (SrvReq *r : s->ring)
+        if (r && r->state == R_TAIL) waiting = true;
+    const bool busy = s->loop_launched && cudaEventQuery(s->loop_done) == cudaErrorNotReady;
+    if (waiting && busy) {
+        if (!s->yielding) {
+            cudaMemcpyAsync(&s->state->yield, &s->h_yield[0], sizeof(int32_t), cudaMemcpyHostToDevice, s->pub_stream);
+            s->yielding = true;
+        }
+        return;
+    }
+    if (waiting) {
+        cudaEvent_t pub;
+        cudaEventCreateWithFlags(&pub, cudaEventDisableTiming);
+        cudaEventRecord(pub, s->pub_stream);
+        cudaStreamWaitEvent(s->loop_stream, pub, 0);
+        cudaEventDestroy(pub);
+        for (int slot = 0; slot < s->nslots; slot++) {
+            SrvReq *r = s->ring[slot];
+            if (!r || r->state != R_TAIL) continue;
+            cudaError_t e = (cudaError_t)chi2_tail(s->ctx, r->req.cat, r->dev, s->loop_stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&s->h_chi[2 * slot], r->dev.chi2, sizeof(double), cudaMemcpyDeviceToHost,
+                                    s->loop_stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&s->h_chi[2 * slot + 1], r->dev.found, 2 * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, s->loop_stream);
+            if (e == cudaSuccess && !r->copied) e = cudaEventCreateWithFlags(&r->copied, cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventRecord(r->copied, s->loop_stream);
+            if (e != cudaSuccess) {
+                set_error(s->ctx, "chi2 delensing: %s", cudaGetErrorString(e));
+                finish(s, r, LT_ERR_CUDA);
+                continue;
+            }
+            r->state = R_COPYING;
+        }
+    }
+    if (!busy && s->yielding) {
+        cudaMemcpyAsync(&s->state->yield, &s->h_yield[1], sizeof(int32_t), cudaMemcpyHostToDevice, s->pub_stream);
+        s->yielding = false;
+    }
 }
 
 /* Keep the persistent kernel running while requests are in flight. */
@@ -251,7 +348,7 @@ void keep_loop(lt_server *s)
     bool running_req = false;
     for (SrvReq *r : s->ring)
         if (r && r->state == R_RUNNING) running_req = true;
-    if (!running_req) return;
+    if (!running_req || s->yielding) return; /* a yield is cleared by run_tails first */
     if (s->loop_launched) {
         const cudaError_t e = cudaEventQuery(s->loop_done);
         if (e == cudaErrorNotReady) return;
@@ -280,6 +377,9 @@ void keep_loop(lt_server *s)
     q.window = s->window;
     q.idle_polls = s->idle_polls;
     q.status = s->ctx->status;
+    /* a new launch starts with no CTA idle and no yield pending (the last launch may have
+     * left together on idle, setting yield from the device) */
+    cudaMemsetAsync(&s->state->yield, 0, 2 * sizeof(int32_t), s->pub_stream);
     /* the published count and descriptors reach the device before the kernel starts */
     cudaEvent_t pub;
     cudaEventCreateWithFlags(&pub, cudaEventDisableTiming);
@@ -323,6 +423,7 @@ void scheduler(lt_server *s)
         }
         const bool done = collect(s);
         if (s->broken == LT_OK) admit(s);
+        if (s->broken == LT_OK) run_tails(s);
         if (s->broken == LT_OK) keep_loop(s);
         if (done) s->cv_done.notify_all();
         const bool busy = s->inflight > 0 || !s->pending.empty();
@@ -378,6 +479,8 @@ lt_status lt_server_create(lt_context *ctx, const lt_server_config *cfg, lt_serv
     if (e == cudaSuccess)
         e = cudaHostAlloc((void **)&s->h_pub, sizeof(unsigned long long) * (size_t)s->nslots, 0);
     if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->h_status, 16 + sizeof(QState), 0);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->h_chi, 2 * sizeof(double) * (size_t)s->nslots, 0);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&s->h_yield, 2 * sizeof(int32_t), 0);
     if (e == cudaSuccess)
         e = cudaHostAlloc((void **)&s->h_flags, sizeof(uint32_t) * (size_t)s->nslots, cudaHostAllocMapped);
     if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&s->d_flags, s->h_flags, 0);
@@ -389,6 +492,8 @@ lt_status lt_server_create(lt_context *ctx, const lt_server_config *cfg, lt_serv
         if (s->h_slots) cudaFreeHost(s->h_slots);
         if (s->h_pub) cudaFreeHost(s->h_pub);
         if (s->h_status) cudaFreeHost(s->h_status);
+        if (s->h_chi) cudaFreeHost(s->h_chi);
+        if (s->h_yield) cudaFreeHost(s->h_yield);
         if (s->h_flags) cudaFreeHost(s->h_flags);
         dev_free(ctx, s->arena_mem, arena_bytes);
         dev_free(ctx, mem, s->dev_bytes);
@@ -396,6 +501,9 @@ lt_status lt_server_create(lt_context *ctx, const lt_server_config *cfg, lt_serv
         return cuda_fail(ctx, e, "server setup");
     }
     memset(s->h_flags, 0, sizeof(uint32_t) * (size_t)s->nslots);
+    memset(s->h_chi, 0, 2 * sizeof(double) * (size_t)s->nslots);
+    s->h_yield[0] = 1;
+    s->h_yield[1] = 0;
     s->ring.assign((size_t)s->nslots, nullptr);
     s->blocks = queue_blocks(s->mode, ctx->num_sms);
     {
@@ -450,6 +558,98 @@ lt_status lt_server_submit(lt_server *s, const lt_request *req, uint64_t *ticket
     s->stats.submitted++;
     *ticket = r->ticket;
     s->cv_work.notify_one();
+    return LT_OK;
+}
+
+lt_status lt_server_submit_chi2(lt_server *s, const lt_catalog *cat, const lt_frame *frame, int32_t n,
+                                const lt_image_systems *sys, uint64_t *ticket)
+{
+    if (!s || !cat || !frame || !ticket) return LT_ERR_INVALID_ARGUMENT;
+    *ticket = 0;
+    lt_context *ctx = s->ctx;
+    if (!(n >= 2 && std::isfinite(frame->xmin) && std::isfinite(frame->xmax) && std::isfinite(frame->ymin) &&
+          std::isfinite(frame->ymax) && frame->xmax > frame->xmin && frame->ymax > frame->ymin &&
+          (long)n * n <= (1L << 31))) {
+        set_error(ctx, "chi2 request: invalid frame or grid size");
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    lt_status st = check_systems(ctx, sys);
+    if (st != LT_OK) return st;
+    if ((size_t)24 * sys->nsystems > 48 * 1024) {
+        set_error(ctx, "chi2 request: at most %d systems", 48 * 1024 / 24);
+        return LT_ERR_INVALID_ARGUMENT;
+    }
+    SrvReq *r = new (std::nothrow) SrvReq();
+    if (!r) return LT_ERR_OUT_OF_MEMORY;
+    r->kind = K_CHI2;
+    r->t_submit = Clock::now();
+    r->frame = *frame;
+    r->n = n;
+    r->nimg.assign(sys->nimages, sys->nimages + sys->nsystems);
+    r->first.resize((size_t)sys->nsystems);
+    int total = 0;
+    for (int i = 0; i < sys->nsystems; i++) {
+        r->first[i] = total;
+        total += sys->nimages[i];
+    }
+    r->ix.assign(sys->x, sys->x + total);
+    r->iy.assign(sys->y, sys->y + total);
+    r->dr.assign(sys->dlsds, sys->dlsds + sys->nsystems);
+    r->chi_bytes = chi2_layout(sys->nsystems, total, frame, n, nullptr, r->dev);
+    /* the deflection grid of the chi2, served by the loop like a map request */
+    lt_request &g = r->req;
+    memset(&g, 0, sizeof(g));
+    g.cat = cat;
+    g.dlsds = 1.0;
+    g.mult = 1.0;
+    g.scale = 1.0;
+    g.nmaps = 2;
+    g.maps[0].kind = LT_MAP_DEFLECTION_X;
+    g.maps[1].kind = LT_MAP_DEFLECTION_Y;
+    g.grid = {frame->xmin, frame->ymin, (frame->xmax - frame->xmin) / (n - 1), (frame->ymax - frame->ymin) / (n - 1),
+              n, n, 0, 0};
+    double *probe[LT_MAX_MAPS];
+    for (int i = 0; i < LT_MAX_MAPS; i++) probe[i] = (double *)s->arena_mem;
+    QItem tmp;
+    st = make_queue_item(ctx, &g, s->precision, probe, &tmp);
+    if (st == LT_OK && r->chi_bytes > s->arena.size()) {
+        set_error(ctx, "chi2 request needs %zu bytes; the server's arena holds %zu", r->chi_bytes, s->arena.size());
+        st = LT_ERR_BUDGET;
+    }
+    if (st != LT_OK) {
+        delete r;
+        return st;
+    }
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->broken != LT_OK || s->stopping) {
+        delete r;
+        return s->broken != LT_OK ? s->broken : LT_ERR_INVALID_ARGUMENT;
+    }
+    r->ticket = s->next_ticket++;
+    s->reqs[r->ticket] = r;
+    s->pending.push_back(r);
+    s->stats.submitted++;
+    *ticket = r->ticket;
+    s->cv_work.notify_one();
+    return LT_OK;
+}
+
+lt_status lt_server_chi2_result(lt_server *s, uint64_t ticket, double *chi2, int32_t *images_found)
+{
+    if (!s || !chi2) return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end() || it->second->kind != K_CHI2) return LT_ERR_INVALID_ARGUMENT;
+    const SrvReq *r = it->second;
+    if (r->state == R_FAILED) return r->status;
+    if (r->state != R_DONE) return LT_ERR_NOT_READY;
+    *chi2 = r->chi2;
+    if (images_found) *images_found = r->found;
+    if (r->overflow) {
+        set_error(s->ctx, "a source had more than %d predicted images (the first %d were used)", LT_MAX_IMAGES,
+                  LT_MAX_IMAGES);
+        return LT_ERR_QUEUE_FULL;
+    }
     return LT_OK;
 }
 
@@ -559,6 +759,8 @@ lt_status lt_server_destroy(lt_server *s)
     cudaFreeHost(s->h_slots);
     cudaFreeHost(s->h_pub);
     cudaFreeHost(s->h_status);
+    cudaFreeHost(s->h_chi);
+    cudaFreeHost(s->h_yield);
     cudaFreeHost(s->h_flags);
     std::vector<lt_catalog *> deferred;
     {

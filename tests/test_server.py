@@ -151,3 +151,49 @@ def test_server_idle_exit_and_relaunch(ctx):
         torch.cuda.synchronize()
         assert np.array_equal(o1["kappa"].cpu().numpy(), exp)
         assert np.array_equal(o2["kappa"].cpu().numpy(), exp)
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64"])
+def test_server_chi2_requests_in_a_mix(ctx, precision):
+    """chi2 requests interleaved with map requests: each chi2 and predicted-image count
+    equals lt_chi2_batch_precision's in the same precision (the grid is served by the loop
+    with the same per-pixel arithmetic; the delensing and chi2 are the same kernels), and
+    the map results are unchanged by the loop's yields for the delensing."""
+    import torch
+    from lenstool_hpc_b200.images import generate_systems
+    frame = (-100., 100., -100., 100.)
+    base = catalog.cluster_galaxy_catalog(2, 198, 20261203)
+    dbase = ctx.upload(base)
+    ic = int(np.argmax(base.b0))
+    systems = generate_systems(lambda bx, by, dr: ctx.delense(dbase, frame, 1024, bx, by, dr), 12, 31, dr=0.6,
+                               centre=(base.position_x[ic], base.position_y[ic]), source_radius=8.)
+    rng = np.random.Generator(np.random.PCG64(17))
+    models = [dbase] + [ctx.upload(catalog.perturb_catalog(base, rng)) for _ in range(3)]
+    sizes = [512, 1024, 256, 768]
+    expect = [ctx.chi2(m, frame, n, systems, precision=precision) for m, n in zip(models, sizes)]
+    cats, work = _mixed(ctx, 8, 5)
+    D, scale = 0.55, 1.7
+    exp_maps = [_alone(ctx, c, g, kinds, precision, D, scale) for c, g, kinds in work]
+    with ctx.server(precision=precision, slots=8, window=4) as srv:
+        outs = [{k: torch.full((g.ny, g.nx), np.nan, dtype=torch.float64, device="cuda") for k in kinds}
+                for c, g, kinds in work]
+        torch.cuda.synchronize()
+        map_t, chi_t = [], []
+        for i, ((c, g, kinds), o) in enumerate(zip(work, outs)):
+            map_t.append(srv.submit(lt.Request(c, g, o, dlsds=D, scale=scale)))
+            if i % 2 == 0:
+                k = i // 2
+                chi_t.append(srv.submit_chi2(models[k], frame, sizes[k], systems))
+        for t in map_t + chi_t:
+            srv.wait(t, 300.)
+        st = srv.stats()
+        assert st["completed"] == len(map_t) + len(chi_t) and st["failed"] == 0
+        for t, (chi, found) in zip(chi_t, expect):
+            got, gfound = srv.chi2_result(t)
+            assert gfound == found and got == chi, (precision, got, chi, gfound, found)
+        torch.cuda.synchronize()
+        for i, (o, exp) in enumerate(zip(outs, exp_maps)):
+            for k, v in o.items():
+                assert plane_close(v.cpu().numpy(), exp[k], k, precision), (precision, i, k)
+        with pytest.raises(lt.LensError):
+            srv.chi2_result(map_t[0])  # not a chi2 ticket
