@@ -439,11 +439,13 @@ double lt_measure_fma_peak(int fp32, int device);
  * reference. */
 int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt);
 
-/* The same for the FP32 atan2 and square root of the compensated pair loops: atan2(y, x)
- * by the library's own polynomial (atan2_own) and by CUDA's atan2f (atan2_cuda), and the
- * approximate square root of x (sqrt_own), on n host inputs (0 = LT_OK). */
+/* The same for the FP32 atan2, square root and atanh of the compensated pair loops:
+ * atan2(y, x) by the library's own polynomial (atan2_own) and by CUDA's atan2f
+ * (atan2_cuda), the approximate square root of x (sqrt_own), and atanh(y) by the
+ * polynomial the deflection and potential use for |y| <= 1/3 (atanh_own), on n host
+ * inputs (0 = LT_OK). */
 int lt_eval_fast_math32(int device, int n, const float *y, const float *x, float *atan2_own, float *atan2_cuda,
-                        float *sqrt_own);
+                        float *sqrt_own, float *atanh_own);
 
 const char *lt_status_string(lt_status status);
 /* Last error message recorded by the context (never NULL). */

@@ -131,17 +131,7 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
             const float dv = v[k] - r.singv;
             near |= (rr < r.rnear2) | (u[k] * u[k] + dv * dv < r.sing_r2) | (rr < r.core_r2);
         }
-        if (OP & OP_POT) {
-            if (r.rnear2 == kProxy64) { /* an FP64 proxy record: every term in FP64 */
-                const lt_rec64 &r64 = recs64[r.idx64];
-#pragma unroll
-                for (int k = 0; k < P; k++) pot_pair_fast<TYPE>(r64, px[k], py, acc.psi[k]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < P; k++) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
-            }
-        }
-        if (!(OP & (OP_HESS | OP_GRAD))) continue;
+        /* the FP64 fallback regions (an FP64 proxy record has rnear2 = +inf: every pixel) */
         if (__any_sync(0xffffffffu, near)) {
             const lt_rec64 &r64 = recs64[r.idx64];
             const double w = kmap ? r64.w : 1.0;
@@ -155,6 +145,7 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
                     acc.hxy[k] = hh.xy;
                 }
                 if (OP & OP_GRAD) grad_pair<TYPE>(r64, px[k], py, acc.gx[k], acc.gy[k]);
+                if (OP & OP_POT) pot_pair_fast<TYPE>(r64, px[k], py, acc.psi[k]);
             }
         } else {
             const float w = kmap ? r.w : 1.0f;
@@ -173,6 +164,7 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
                     kahan_add(acc.gxs[k], acc.gxc[k], t.x * r.cs - t.y * r.sn);
                     kahan_add(acc.gys[k], acc.gyc[k], t.y * r.cs + t.x * r.sn);
                 }
+                if (OP & OP_POT) kahan_add(acc.ps[k], acc.pc[k], pot32<TYPE>(r, u[k], v[k]));
             }
         }
     }

@@ -1,7 +1,7 @@
 /*
  * lt_halo.h -- device layout of a packed halo catalogue (shared by host and device code).
  *
- * Each halo becomes one 192-byte record of per-halo invariants, so that the per-pair
+ * Each halo becomes one 256-byte record of per-halo invariants, so that the per-pair
  * work of the grid kernels starts from the pixel offset.  The invariants are the
  * sub-expressions the reference recomputes for every pixel (src/gradient.cpp:744-811,
  * src/gradient2.cpp:54-83, src/potential_GPU.cu:47-72), evaluated once with the same
@@ -16,7 +16,10 @@
  *     pref_g = ci * b0 * rcut/(rcut - rc)  (81) | ci * b0  (8)      -- deflection
  *     pref_h = ci * b0 * rcut/(rcut - rc)  (81) | ci * b0  (8)      -- Hessian, potential
  *     rc2 = rc^2, rcut2 = rcut^2, tsr_c = 2 rc sqrt(eps), tsr_t = 2 rcut sqrt(eps),
- *     e1 = 2 sqrt(eps)/(1-eps), e2 = 2 sqrt(eps)/(1+eps)
+ *     e1 = 2 sqrt(eps)/(1-eps), e2 = 2 sqrt(eps)/(1+eps),
+ *     dr2 = rc^2 - rcut^2, drs = rc - rcut, om2 = (1-eps)^2, e4cxi = 4 eps/(1+eps)^2,
+ *     ok3c = (1-eps)(3+eps) rc, ok3t = (1-eps)(3+eps) rcut, i4rc2 = 1/(4 rc^2),
+ *     i4rcut2 = 1/(4 rcut^2)  (the deflection-based potential of lt_profiles64.cuh)
  *   type 5 (SIS): cx1 = 1-eps, cx1inv = 1+eps, pref_g = (1-eps) b0,
  *     pref_h = (1+eps) b0, ci = b0 (1-eps)(1+eps)
  *   all: w = dlsds (Kmap weight), type in `type`.
@@ -37,8 +40,10 @@ struct alignas(16) lt_rec64 {
     double cyro_inv, ci, pref_g, pref_h;
     double rc2, rcut2, tsr_c, tsr_t;
     double e1, e2, w, k4;
+    double dr2, drs, om2, e4cxi;
+    double ok3c, ok3t, i4rc2, i4rcut2;
 };
-static_assert(sizeof(lt_rec64) == 192, "record size");
+static_assert(sizeof(lt_rec64) == 256, "record size");
 
 /* A chunk: a run of consecutive halos of one type, at most LT_CHUNK halos long.  The
  * grid kernels walk the chunk list; runs of equal type are the reference's dispatch unit

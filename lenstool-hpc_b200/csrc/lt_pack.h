@@ -98,6 +98,14 @@ LT_HD inline void pack64(int t, double x, double y, double cs, double sn, double
     r.tsr_t = mul(mul(2., rcut), sqe);
     r.e1 = div(mul(2., sqe), sub(1, e));
     r.e2 = div(mul(2., sqe), add(1, e));
+    r.dr2 = mul(sub(rc, rcut), add(rc, rcut));
+    r.drs = sub(rc, rcut);
+    r.om2 = mul(sub(1., e), sub(1., e));
+    r.e4cxi = div(mul(4., e), mul(add(1., e), add(1., e)));
+    r.ok3c = mul(mul(sub(1., e), add(3., e)), rc);
+    r.ok3t = mul(mul(sub(1., e), add(3., e)), rcut);
+    r.i4rc2 = div(1., mul(4., mul(rc, rc)));
+    r.i4rcut2 = div(1., mul(4., mul(rcut, rcut)));
 }
 
 /* module_readParameters_calculatePotentialparameter_SOA (src/module_readParameters.cpp:
@@ -195,10 +203,12 @@ LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     o.gpre = f32(mul(mul(mul(0.5, ci), r.b0), t05));
     o.kpre = f32(type == 81 ? mul(mul(-0.5, r.b0), t05) : mul(0.5, r.b0));
     o.ppre = f32(mul(mul(ci, r.b0), t05));
-    o.e1 = f32(div(mul(2., sqe), sub(1., e)));
-    o.e2 = f32(div(mul(2., sqe), add(1., e)));
-    o.irc = f32(div(1., r.rc));
-    o.ircut = f32(div(1., r.rcut));
+    o.om2 = f32(mul(sub(1., e), sub(1., e)));
+    o.e4cxi = f32(div(mul(4., e), mul(add(1., e), add(1., e))));
+    o.ok3c = f32(mul(mul(sub(1., e), add(3., e)), r.rc));
+    o.ok3t = f32(mul(mul(sub(1., e), add(3., e)), r.rcut));
+    o.i4rc2 = f32(div(1., mul(4., mul(r.rc, r.rc))));
+    o.i4rcut2 = f32(div(1., mul(4., mul(r.rcut, r.rcut))));
     const double sr = type == 81 ? r.rcut : r.rc;
     o.singv = f32(mul(mul(2., sr), sqe));
     const double srad = mul(add(kSingFrac, mul(kSingEps, e)), sr);

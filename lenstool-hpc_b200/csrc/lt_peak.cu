@@ -104,33 +104,37 @@ extern "C" int lt_eval_fast_math(int device, int n, const double *x, double *rcp
 #include "lt_profiles32.cuh"
 
 namespace {
-__global__ void fast_math32_kernel(const float *y, const float *x, float *own, float *cuda, float *sq, int n)
+__global__ void fast_math32_kernel(const float *y, const float *x, float *own, float *cuda, float *sq, float *th,
+                                   int n)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         own[i] = lt::fatan2(y[i], x[i]);
         cuda[i] = atan2f(y[i], x[i]);
         sq[i] = lt::fsqrt(x[i]);
+        th[i] = lt::fatanh_third(y[i]);
     }
 }
 } // namespace
 
 extern "C" int lt_eval_fast_math32(int device, int n, const float *y, const float *x, float *atan2_own,
-                                   float *atan2_cuda, float *sqrt_own)
+                                   float *atan2_cuda, float *sqrt_own, float *atanh_own)
 {
-    if (n < 1 || !y || !x || !atan2_own || !atan2_cuda || !sqrt_own) return 1;
+    if (n < 1 || !y || !x || !atan2_own || !atan2_cuda || !sqrt_own || !atanh_own) return 1;
     if (cudaSetDevice(device) != cudaSuccess) return 4;
     float *d = nullptr;
     const size_t b = sizeof(float) * (size_t)n;
-    if (cudaMalloc(&d, 5 * b) != cudaSuccess) return 5;
+    if (cudaMalloc(&d, 6 * b) != cudaSuccess) return 5;
     cudaError_t e = cudaMemcpy(d, y, b, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d + n, x, b, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
-        fast_math32_kernel<<<256, 256>>>(d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, d + 4 * (size_t)n, n);
+        fast_math32_kernel<<<256, 256>>>(d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, d + 4 * (size_t)n,
+                                         d + 5 * (size_t)n, n);
         lt::count_launch(1);
         e = cudaMemcpy(atan2_own, d + 2 * (size_t)n, b, cudaMemcpyDeviceToHost);
     }
     if (e == cudaSuccess) e = cudaMemcpy(atan2_cuda, d + 3 * (size_t)n, b, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(sqrt_own, d + 4 * (size_t)n, b, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(atanh_own, d + 5 * (size_t)n, b, cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? 0 : 4;
 }

@@ -35,9 +35,10 @@ struct alignas(16) lt_rec32 {
     float gpre, rc, rcut, drs;    /* gamma prefactor, rc, rcut, rc - rcut                    */
     float dr2, rc2, rcut2, w;     /* rc^2 - rcut^2, rc^2, rcut^2, Kmap weight                */
     float rnear2, singv, sing_r2, core_r2; /* FP64 fallback regions (squared radii)          */
-    float cpi, s2rc, s2rcut, irc; /* cx1 + 1/cx1, 2 sqrt(e) rc, 2 sqrt(e) rcut, 1/rc           */
-    float e1, e2, ppre, ircut;    /* potential: 2 sqrt(e)/(1-e), 2 sqrt(e)/(1+e), prefactor, 1/rcut */
-    int32_t type, idx64, pad0, pad1;
+    float cpi, s2rc, s2rcut, ok3c; /* cx1 + 1/cx1, 2 sqrt(e) rc, 2 sqrt(e) rcut, (1-e)(3+e) rc */
+    float om2, e4cxi, ppre, i4rc2; /* potential: (1-e)^2, 4e/(1+e)^2, prefactor, 1/(4 rc^2)    */
+    int32_t type, idx64;
+    float ok3t, i4rcut2;           /* (1-e)(3+e) rcut, 1/(4 rcut^2)                             */
 };
 static_assert(sizeof(lt_rec32) == 160, "record size");
 
@@ -84,6 +85,20 @@ __device__ __forceinline__ float fatan2(float y, float x)
     r = ay > ax ? 1.57079637f - r : r;
     r = x < 0.f ? 3.14159274f - r : r;
     return copysignf(r, y);
+}
+
+/* atanh s for |s| <= 1/3: s P(s^2), P = 1 + c1 x + ... + c4 x^4 fitted to atanh(sqrt x)/sqrt x
+ * on [0, 1/9] by a Remez exchange on the relative error (4.5e-9 in exact arithmetic; 1.2e-7
+ * relative evaluated in FP32).  log1p(t)/2 = atanh(t/(2 + t)). */
+__device__ __forceinline__ float fatanh_third(float s)
+{
+    const float x = s * s;
+    float p = 1.400599331e-01f;
+    p = fmaf(p, x, 1.400090307e-01f);
+    p = fmaf(p, x, 2.001076341e-01f);
+    p = fmaf(p, x, 3.333320916e-01f);
+    p = fmaf(p, x, 1.0f);
+    return s * p;
 }
 
 struct KG32 {
@@ -177,34 +192,51 @@ struct G32 {
  * of the core and cut terms, which cancel far from the halo.  Here that difference is
  * log(z_c/z_t) = log(1 + eps) with eps = (dN D_t - dD N_t)/(D_c N_t), built from the exact
  * differences dN = N_c - N_t = i 2 sqrt(e) (w_c - w_t), w_c - w_t = (rc^2 - rcut^2)/(w_c + w_t),
- * and dD = i 2 sqrt(e) (rc - rcut): no digit is lost to the cancellation, and
- * Re log(1 + eps) = log1p(2 eps_r + |eps|^2)/2, Im = atan2(eps_i, 1 + eps_r).  (The
- * reference's two arguments never straddle the branch cut here: arg z_c - arg z_t equals
- * arg(z_c/z_t), checked over the workload catalogues.)  SIS (src/gradient.cpp:260-299):
+ * and dD = i 2 sqrt(e) (rc - rcut): no digit is lost to the cancellation.  With
+ * eps = num/den, A = |den + num|^2 and B = |den|^2 (A - B = 2 Re(num conj den) + |num|^2
+ * taken directly), Re log(1 + eps) = log(A/B)/2 = atanh((A - B)/(A + B)) (fatanh_third
+ * where |s| <= 1/3, i.e. A/B in [1/2, 2]; __logf(A/B)/2 outside, where it is good to a
+ * few ulp), and Im log(1 + eps) = atan2(Im(num conj den), B + Re(num conj den)), the
+ * scale |den|^-2 dropped from both arguments.  (The reference's two arguments never
+ * straddle the branch cut here: arg z_c - arg z_t equals arg(z_c/z_t), checked over
+ * random halos down to 1e-3 rc from the centre.)  SIS (src/gradient.cpp:260-299):
  * b0 ((1-e) u, (1+e) v)/sqrt((1-e) u^2 + (1+e) v^2). */
+struct Log32 {
+    float li, lr;       /* arg and log| | of z (PIEMD) or z_c/z_t (dPIE) */
+    float rho2, wc, wt; /* rho^2, w_c, w_t (w_t: dPIE only) */
+};
+
 template <int TYPE>
-__device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
+__device__ __forceinline__ Log32 log32(const lt_rec32 &h, float u, float v)
 {
-    if (TYPE == 5) {
-        const float ir = rsqrtf(u * u * h.cx1 + v * v * h.icx1);
-        return {h.ppre * h.cx1 * u * ir, h.ppre * h.icx1 * v * ir};
-    }
-    const float rho2 = u * u * h.cxi + v * v * h.cyi;
-    const float xc = h.rc2 + rho2;
-    const float wc = xc * rsqrtf(xc);
+    Log32 o;
+    o.rho2 = u * u * h.cxi + v * v * h.cyi;
+    const float xc = h.rc2 + o.rho2;
+    o.wc = xc * rsqrtf(xc);
     const float nr = h.cx1 * u;
     const float dci = h.s2rc - v;
     if (TYPE == 8) {
-        const float nci = h.s2 * wc - v * h.icx1;
-        /* z = N/D: log|z| = (log|N|^2 - log|D|^2)/2, arg z = arg(N conj(D)) */
-        const float lr = 0.5f * __logf((nr * nr + nci * nci) * frcp(u * u + dci * dci));
-        const float li = fatan2(nci * u - nr * dci, nr * u + nci * dci);
-        return {h.ppre * li, -h.ppre * lr};
+        const float nci = h.s2 * o.wc - v * h.icx1;
+        /* z = N/D, A = |N|^2, B = |D|^2: log|z| = atanh((A - B)/(A + B)), where (with
+         * w_c^2 - rc^2 = rho^2) A - B = 2 v (4e v/(1-e)^2 - 2 sqrt(e) (w_c/cx1 - rc)) is taken
+         * without the cancellation of |N|^2 - |D|^2 near |z| = 1 (small e); arg z =
+         * arg(N conj(D)), whose imaginary part u (2 sqrt(e) (w_c - cx1 rc) - v (1/cx1 - cx1))
+         * avoids the same cancellation (1/cx1 - cx1 = 4e/(1-e^2)) */
+        const float A = nr * nr + nci * nci, B = u * u + dci * dci;
+        const float amb = 2.f * v * (h.e4 * h.cyi * v - h.s2 * fmaf(o.wc, h.icx1, -h.rc));
+        const float apb = A + B;
+        const float rs = frcp(apb);
+        const float s0 = amb * rs;
+        const float s = fmaf(rs, fmaf(-s0, apb, amb), s0);
+        o.lr = fabsf(s) <= (1.f / 3.f) ? fatanh_third(s) : 0.5f * __logf(A * frcp(B));
+        o.li = fatan2(u * (h.s2 * fmaf(-h.cx1, h.rc, o.wc) - v * (h.e4 * h.ome2)), nr * u + nci * dci);
+        o.wt = 0.f;
+        return o;
     }
-    const float xt = h.rcut2 + rho2;
-    const float wt = xt * rsqrtf(xt);
-    const float dw = h.dr2 * frcp(wc + wt);
-    const float nti = h.s2 * wt - v * h.icx1;
+    const float xt = h.rcut2 + o.rho2;
+    o.wt = xt * rsqrtf(xt);
+    const float dw = h.dr2 * frcp(o.wc + o.wt);
+    const float nti = h.s2 * o.wt - v * h.icx1;
     const float dti = h.s2rcut - v;
     const float dni = h.s2 * dw, ddi = h.s2 * h.drs;
     /* num = i dni D_t - i ddi N_t,  den = D_c N_t */
@@ -212,97 +244,68 @@ __device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
     const float numi = dni * u - ddi * nr;
     const float denr = u * nr - dci * nti;
     const float deni = u * nti + dci * nr;
-    const float inv = frcp(denr * denr + deni * deni);
-    const float er = (numr * denr + numi * deni) * inv;
-    const float ei = (numi * denr - numr * deni) * inv;
-    const float lr = 0.5f * log1pf(er * (2.f + er) + ei * ei);
-    const float li = fatan2(ei, 1.f + er);
-    return {h.ppre * li, -h.ppre * lr};
+    /* 1 + eps = (den + num)/den; c + i d = num conj(den), B = |den|^2, A = |den + num|^2 */
+    const float c = numr * denr + numi * deni;
+    const float d = numi * denr - numr * deni;
+    const float B = denr * denr + deni * deni;
+    const float amb = fmaf(2.f, c, numr * numr + numi * numi); /* A - B */
+    const float apb = fmaf(2.f, B, amb);                       /* A + B */
+    const float rs = frcp(apb);
+    const float s0 = amb * rs;
+    const float s = fmaf(rs, fmaf(-s0, apb, amb), s0); /* (A - B)/(A + B), one correction step */
+    o.lr = fabsf(s) <= (1.f / 3.f) ? fatanh_third(s) : 0.5f * __logf((B + amb) * frcp(B));
+    o.li = fatan2(d, B + c);
+    return o;
 }
 
-/* Potential, FP32.  pi05 of src/potential_GPU.cu:47-72 is, with b1 = cosh(eta + zeta),
- * b2 = cosh(eta - zeta) (zeta real), r (Im k u - Re k v) b0 ci/rho_e with
- *   k = sinh(2 eta) log(cosh^2 eta/(b1 b2)) + sinh(2 zeta) log(b1/b2).
- * Writing w = tanh eta tanh zeta and a = eta_re,
- *   b1 b2 = cosh^2 eta cosh^2 zeta (1 - w)(1 + w),   b1/b2 = (1 + w)/(1 - w),
- *   1 +- w = N+- / (cosh 2a + cos 2 eta_im),
- *   N+  = (e^{2a}  - 2 sinh 2a/(rho + 1) + cos 2 eta_im) + i B,
- *   N-  = (e^{-2a} + 2 sinh 2a/(rho + 1) + cos 2 eta_im) - i B,   B = tanh zeta sin 2 eta_im,
- * whose real parts are sums of positive terms or lose at most half (no cancellation, also
- * where tanh eta -> +-1 at high ellipticity), so
- *   log(b1/b2) = log|N+|^2/|N-|^2 / 2 + i arg(N+ conj N-),
- *   log(cosh^2 eta/(b1 b2)) = -log(cosh^4 zeta |N+|^2 |N-|^2/(cosh 2a + cos 2 eta_im)^4)/2
- *                             - i arg(N+ N-),
- * with Re(N+ N-) = Re N+ Re N- + B^2 > 0 and Im(N+ N-) = -2 B tanh zeta sinh 2a exactly;
- * the arguments are those of the reference's principal logarithms (both |arg| < pi), and no
- * complex quotient is formed.  With s = e1 v/z and t = e2 u/z:
- *   e^{2a} = exp(-asinh s) = (|s| + sqrt(s^2 + 1))^(-sign s),
- *   sin 2 eta_im = t, cos 2 eta_im = sqrt(1 - t^2),
- *   e^{2 zeta} = rho = (rho_e + sqrt(r^2 + rho_e^2))/r, with rho - 1 taken without
- *   cancellation as (rho_e + rho_e^2/(sqrt(r^2 + rho_e^2) + r))/r,
- *   tanh zeta = (rho - 1)/(rho + 1), cosh^2 zeta = (rho + 1)^2/(4 rho),
- *   sinh 2 zeta = (rho - 1)(rho + 1)/(2 rho).
- * Returns the halo's potential without the FP64 cluster terms; far from the halo the
- * core - cut difference loses ~1e-5 of the term, small against the map's scale. */
-struct Pi05Shared {
-    float sh2r, sh2i;      /* sinh(2 eta) */
-    float E2, iE2, sh2a;   /* e^{2a}, e^{-2a}, sinh 2a */
-    float c2e, t;          /* cos, sin of 2 eta_im */
-    float itd4;            /* (cosh 2a + cos 2 eta_im)^-4 */
-};
-
-__device__ __forceinline__ float pi05_term32(const Pi05Shared &p, float u, float v, float srem, float rem2, float r,
-                                             float r2, float ir)
+template <int TYPE>
+__device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v)
 {
-    const float q = fsqrt(r2 + rem2);
-    const float dm = (srem + rem2 * frcp(q + r)) * ir; /* rho - 1 */
-    const float rho = 1.f + dm, rho1 = rho + 1.f;
-    const float inv = frcp(rho * rho1);
-    const float irho = rho1 * inv, irho1 = rho * inv;
-    const float tz = dm * irho1;                        /* tanh zeta */
-    const float sh2z = 0.5f * dm * rho1 * irho;         /* sinh 2 zeta */
-    const float ch2z = 0.25f * rho1 * rho1 * irho;      /* cosh^2 zeta */
-    const float m = 2.f * irho1 * p.sh2a;
-    const float A = (p.E2 - m) + p.c2e, C = (p.iE2 + m) + p.c2e, B = tz * p.t, B2 = B * B;
-    const float np2 = A * A + B2, nm2 = C * C + B2;
-    const float a2r = 0.5f * __logf(np2 * frcp(nm2));
-    const float a2i = fatan2(B * (A + C), A * C - B2);
-    const float a1r = -0.5f * __logf((ch2z * ch2z) * (np2 * nm2) * p.itd4);
-    const float a1i = fatan2(2.f * B * tz * p.sh2a, A * C + B2);
-    const float kr = (p.sh2r * a1r - p.sh2i * a1i) + sh2z * a2r;
-    const float ki = (p.sh2i * a1r + p.sh2r * a1i) + sh2z * a2i;
-    return r * (ki * u - kr * v);
+    if (TYPE == 5) {
+        const float ir = rsqrtf(u * u * h.cx1 + v * v * h.icx1);
+        return {h.ppre * h.cx1 * u * ir, h.ppre * h.icx1 * v * ir};
+    }
+    const Log32 z = log32<TYPE>(h, u, v);
+    return {h.ppre * z.li, -h.ppre * z.lr};
+}
+
+/* log(1 + t)/2 for t >= 0: atanh(t/(2 + t)) by fatanh_third for t <= 1, __logf above
+ * (1 + t >= 2, where it is good to a few ulp). */
+__device__ __forceinline__ float half_log1p_pos(float t)
+{
+    const float s = t * frcp(2.f + t);
+    return t <= 1.f ? fatanh_third(s) : 0.5f * __logf(1.f + t);
+}
+
+/* Potential, FP32, through the deflection.  For a core-softened isothermal ellipsoid the
+ * potential is x . alpha plus one logarithm per core radius, and the reference's pi05
+ * (src/potential_GPU.cu:47-72, PIEMD; the cut dPIE is pref (pi05(rc) - pi05(rcut)),
+ * src/potential_GPU.cu:137-187) is that form with the constant that makes it vanish at the
+ * centre.  In the halo frame, with alpha = ppre (li, -lr) of log32 and w_r = sqrt(r^2 + rho^2):
+ *   psi = ppre [ (u li - v lr) - 2 sqrt(e) (rc H(t_c) - rcut H(t_t)) ],  H(t) = log(1 + t)/2,
+ *   1 + t_r = (((1-e) w_r + (1+e) r)^2 + 4e u^2/(1+e)^2)/(4 r^2),
+ * (PIEMD: the rc term alone), and t_r is taken without cancellation as
+ *   t_r = [(1-e)^2 A_r w_r + (1-e)(3+e) r A_r + 4e u^2/(1+e)^2]/(4 r^2),
+ *   A_r = w_r - r = rho^2/(w_r + r),
+ * a sum of non-negative terms.  (In FP64 the identity holds to rounding against pi05 over
+ * e_pot up to 0.33 and rc/rcut down to 1/150; the tests compare the two paths.)  The form
+ * shares the deflection's singular points, so the kernels take the potential in FP64 in the
+ * same fallback regions as the deflection. */
+__device__ __forceinline__ float tpot32(float rho2, float uterm, float w, float r, float ok3, float i4r2, float om2)
+{
+    const float a = rho2 * frcp(w + r);
+    return (a * fmaf(om2, w, ok3) + uterm) * i4r2;
 }
 
 template <int TYPE>
 __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v)
 {
     if (TYPE == 5) return h.ppre * fsqrt(u * u * h.cx1 + v * v * h.icx1);
-    const float uu = u * u, vv = v * v;
-    const float rem2 = uu * h.cxi + vv * h.cyi;
-    const float irem = rsqrtf(rem2);
-    const float srem = rem2 * irem;
-    const float iz = rsqrtf(uu + vv);
-    const float s = h.e1 * v * iz;
-    const float t = h.e2 * u * iz;
-    const float g = fabsf(s) + fsqrt(s * s + 1.f);
-    const float ig = frcp(g);
-    const float E2 = s >= 0.f ? ig : g, iE2 = s >= 0.f ? g : ig; /* exp(+-2 eta_re) */
-    const float ch2a = 0.5f * (E2 + iE2), sh2a = 0.5f * (E2 - iE2);
-    const float c2e = fsqrt(fmaxf(1.f - t * t, 0.f));
-    Pi05Shared p;
-    p.sh2r = sh2a * c2e;
-    p.sh2i = ch2a * t;
-    p.E2 = E2;
-    p.iE2 = iE2;
-    p.sh2a = sh2a;
-    p.c2e = c2e;
-    p.t = t;
-    const float itd = frcp(ch2a + c2e), itd2 = itd * itd;
-    p.itd4 = itd2 * itd2;
-    float term = pi05_term32(p, u, v, srem, rem2, h.rc, h.rc2, h.irc);
-    if (TYPE == 81) term -= pi05_term32(p, u, v, srem, rem2, h.rcut, h.rcut2, h.ircut);
-    return h.ppre * term * irem;
+    const Log32 z = log32<TYPE>(h, u, v);
+    const float ut = h.e4cxi * u * u;
+    float hs = h.rc * half_log1p_pos(tpot32(z.rho2, ut, z.wc, h.rc, h.ok3c, h.i4rc2, h.om2));
+    if (TYPE == 81) hs -= h.rcut * half_log1p_pos(tpot32(z.rho2, ut, z.wt, h.rcut, h.ok3t, h.i4rcut2, h.om2));
+    return h.ppre * ((u * z.li - v * z.lr) - h.s2 * hs);
 }
 
 /* Kahan compensated accumulation of one FP32 component. */

@@ -254,12 +254,13 @@ __device__ __forceinline__ void pot_pair(const lt_rec64 &h, double px, double py
     psi += h.pref_h * t / srem;
 }
 
-/* The potential in the cancellation-free form derived in lt_profiles32.cuh (pi05 through
- * N+- = (cosh 2a + cos 2 eta_im)(1 +- tanh eta tanh zeta), no complex quotient, no branch
- * wrap), in FP64: per dPIE pair 4 log and 4 atan2 in place of the formula's 16 exp, 6 log,
- * 4 atan2, asinh, asin and 2 sincos.  Against an extended-precision evaluation of pi05 it
- * is within 1e-13 of a term's scale where the reference formula in FP64 is within 2e-13
- * (checked per term over e in [1e-5, 0.73], r in [0.05, 800]). */
+/* pi05 in the cancellation-free N+- form (N+- = (cosh 2a + cos 2 eta_im)(1 +- tanh eta
+ * tanh zeta), no complex quotient, no branch wrap), in FP64: per dPIE pair 4 log and 4 atan2
+ * in place of the formula's 16 exp, 6 log, 4 atan2, asinh, asin and 2 sincos.  Against an
+ * extended-precision evaluation of pi05 it is within 1e-13 of a term's scale where the
+ * reference formula in FP64 is within 2e-13 (checked per term over e in [1e-5, 0.73], r in
+ * [0.05, 800]).  pot_pair_fast uses it only near the points where the cheaper
+ * deflection-based form below loses digits. */
 struct Pi05Shared64 {
     double sh2r, sh2i, E2, iE2, sh2a, c2e, t, itd4;
 };
@@ -288,6 +289,94 @@ __device__ __forceinline__ double pi05_term64(const Pi05Shared64 &p, double u, d
     return r * (ki * u - kr * v);
 }
 
+/* The potential through the deflection (the derivation and the record invariants are
+ * those of pot32 in lt_profiles32.cuh), in FP64 with CUDA's log, log1p and atan2: per dPIE
+ * pair 3 logarithms and 1 atan2.  log64 is the complex logarithm of the PIEMD ratio
+ * z = N/D (TYPE 8) or of z_c/z_t (TYPE 81): as log(1 + eps) in the cancellation-free form
+ * of log32, or, where `split` (near the core radius's 0/0 point, where that form loses
+ * digits on the scale of rcut), as log z_c - log z_t (digits lost on the scale of rc). */
+struct Log64 {
+    double li, lr, wc, wt;
+};
+
+/* log z = log(N/D) of one PIEMD radius r (w = sqrt(r^2 + rho^2), tsr = 2 sqrt(e) r): |z|^2
+ * straight from |N|^2/|D|^2, and arg z = arg(N conj D) with the imaginary part
+ * u (2 sqrt(e) (w - cx1 r) - v (1/cx1 - cx1)) (1/cx1 - cx1 = 4e/(1-e^2) = e1 e2), free of the
+ * cancellation of its two products for small e. */
+__device__ __forceinline__ void piemd_log64(const lt_rec64 &h, double u, double v, double uu, double w, double r,
+                                            double tsr, double &li, double &lr)
+{
+    const double nr = h.cx1 * u;
+    const double nci = h.sqe2 * w - v * h.cx1inv;
+    const double dci = tsr - v;
+    lr = 0.5 * log((nr * nr + nci * nci) * rcp64(uu + dci * dci));
+    li = atan2(u * (h.sqe2 * fma(-h.cx1, r, w) - v * (h.e1 * h.e2)), nr * u + nci * dci);
+}
+
+template <int TYPE>
+__device__ __forceinline__ Log64 log64(const lt_rec64 &h, double u, double v, double uu, double rho2, bool split)
+{
+    Log64 o;
+    const double xc = h.rc2 + rho2;
+    o.wc = xc * rsqrt64(xc);
+    if (TYPE == 8) {
+        piemd_log64(h, u, v, uu, o.wc, h.rc, h.tsr_c, o.li, o.lr);
+        o.wt = 0.;
+        return o;
+    }
+    const double xt = h.rcut2 + rho2;
+    o.wt = xt * rsqrt64(xt);
+    if (split) {
+        double li_t, lr_t;
+        piemd_log64(h, u, v, uu, o.wc, h.rc, h.tsr_c, o.li, o.lr);
+        piemd_log64(h, u, v, uu, o.wt, h.rcut, h.tsr_t, li_t, lr_t);
+        o.li -= li_t;
+        o.lr -= lr_t;
+        return o;
+    }
+    const double nr = h.cx1 * u;
+    const double dci = h.tsr_c - v;
+    const double dw = h.dr2 * rcp64(o.wc + o.wt);
+    const double nti = h.sqe2 * o.wt - v * h.cx1inv;
+    const double dti = h.tsr_t - v;
+    const double dni = h.sqe2 * dw, ddi = h.sqe2 * h.drs;
+    const double numr = ddi * nti - dni * dti;
+    const double numi = dni * u - ddi * nr;
+    const double denr = u * nr - dci * nti;
+    const double deni = u * nti + dci * nr;
+    const double c = numr * denr + numi * deni;
+    const double d = numi * denr - numr * deni;
+    const double B = denr * denr + deni * deni;
+    o.lr = 0.5 * log1p(fma(2., c, numr * numr + numi * numi) * rcp64(B));
+    o.li = atan2(d, B + c);
+    return o;
+}
+
+template <int TYPE>
+__device__ __forceinline__ double pot64_defl(const lt_rec64 &h, double u, double v, double uu, double rho2,
+                                             bool split)
+{
+    const Log64 z = log64<TYPE>(h, u, v, uu, rho2, split);
+    const double ut = h.e4cxi * uu;
+    double hs = h.rc * log1p((rho2 * rcp64(z.wc + h.rc) * fma(h.om2, z.wc, h.ok3c) + ut) * h.i4rc2);
+    if (TYPE == 81)
+        hs -= h.rcut * log1p((rho2 * rcp64(z.wt + h.rcut) * fma(h.om2, z.wt, h.ok3t) + ut) * h.i4rcut2);
+    return h.pref_h * ((u * z.li - v * z.lr) - 0.5 * h.sqe2 * hs);
+}
+
+/* Zones of pot_pair_fast, as squared radii.  The quotients of the deflection form are 0/0
+ * at u = 0, v = 2 sqrt(e) r and lose ~1e-16 s/distance near those points, s the size of
+ * the terms they are built from.  Measured against an extended-precision pi05 (emulating
+ * these formulas), psi stays within 1e-13 of itself outside
+ *   0.0316 rc of the core point and 0.02 rcut of the cut point (dPIE): there the N+- form
+ *   of pi05_term64 is used (and at the centre itself, where pi05 is 0/0 as the reference's);
+ *   0.02 rcut of the core point (dPIE): there log z_c - log z_t (s = rc), elsewhere
+ *   log(1 + eps) (s = rcut).
+ * (Near the centre the N+- form is only good to ~1e-12 of the small psi there; the
+ * deflection form is regular at the centre.) */
+constexpr double kSingCut64 = 4e-4;  /* x rcut^2 */
+constexpr double kSingCore64 = 1e-3; /* x rc^2 */
+
 template <int TYPE>
 __device__ __forceinline__ void pot_pair_fast(const lt_rec64 &h, double px, double py, double &psi)
 {
@@ -299,6 +388,19 @@ __device__ __forceinline__ void pot_pair_fast(const lt_rec64 &h, double px, doub
         return;
     }
     const double rem2 = uu * h.cxro_inv + vv * h.cyro_inv;
+    const double dvc = v - h.tsr_c;
+    const double dc2 = uu + dvc * dvc;
+    bool sing = (uu + vv == 0.) | (dc2 < kSingCore64 * h.rc2);
+    bool split = false;
+    if (TYPE == 81) {
+        const double dvt = v - h.tsr_t;
+        sing |= uu + dvt * dvt < kSingCut64 * h.rcut2;
+        split = dc2 < kSingCut64 * h.rcut2;
+    }
+    if (!sing) {
+        psi += pot64_defl<TYPE>(h, u, v, uu, rem2, split);
+        return;
+    }
     const double irem = rsqrt64(rem2), srem = rem2 * irem;
     const double iz = rsqrt64(uu + vv);
     const double s = h.e1 * v * iz, t = h.e2 * u * iz;

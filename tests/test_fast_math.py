@@ -38,6 +38,17 @@ def test_rcp_rsqrt_within_few_ulp():
     assert ulp_diff(rsq, ref).max() <= 2
 
 
+def _fast_math32(L, y, x):
+    fp = C.POINTER(C.c_float)
+    L.lt_eval_fast_math32.argtypes = [C.c_int, C.c_int, fp, fp, fp, fp, fp, fp]
+    y = np.ascontiguousarray(y, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    outs = [np.empty(y.size, np.float32) for _ in range(4)]
+    ptr = lambda a: a.ctypes.data_as(fp)  # noqa: E731
+    assert L.lt_eval_fast_math32(0, y.size, ptr(y), ptr(x), *[ptr(o) for o in outs]) == 0
+    return outs  # atan2 (own), atan2f (CUDA), sqrt(x), atanh(y)
+
+
 def test_fp32_atan2_and_sqrt():
     """The FP32 atan2 of the compensated potential (own polynomial) against FP64 atan2 and
     CUDA's atan2f, and its approximate square root against FP64 sqrt, over the operand
@@ -48,17 +59,13 @@ def test_fp32_atan2_and_sqrt():
     from lenstool_hpc_b200 import build
     build.build()
     L = lt.load_library()
-    fp = C.POINTER(C.c_float)
-    L.lt_eval_fast_math32.argtypes = [C.c_int, C.c_int, fp, fp, fp, fp, fp]
     rng = np.random.default_rng(2)
     n = 400000
     y = (rng.standard_normal(n) * 10.0 ** rng.uniform(-6, 3, n)).astype(np.float32)
     x = (rng.standard_normal(n) * 10.0 ** rng.uniform(-6, 3, n)).astype(np.float32)
     y[:4] = [0., -0., 1., -1.]
     x[:4] = [1., -1., 0., 0.]
-    own, cuda, sq = (np.empty(n, np.float32) for _ in range(3))
-    ptr = lambda a: a.ctypes.data_as(fp)  # noqa: E731
-    assert L.lt_eval_fast_math32(0, n, ptr(y), ptr(x), ptr(own), ptr(cuda), ptr(sq)) == 0
+    own, cuda, _, _ = _fast_math32(L, y, x)
     ref = np.arctan2(y.astype(np.float64), x.astype(np.float64))
     err = np.abs(own.astype(np.float64) - ref)
     assert err.max() <= 4e-7
@@ -68,6 +75,24 @@ def test_fp32_atan2_and_sqrt():
     big = ax > 1e-30
     rs = np.sqrt(ax[big].astype(np.float64))
     # sqrt of |x| (the loops take roots of non-negative operands only)
-    sq2 = np.empty(n, np.float32)
-    assert L.lt_eval_fast_math32(0, n, ptr(y), ptr(ax.astype(np.float32)), ptr(own), ptr(cuda), ptr(sq2)) == 0
+    _, _, sq2, _ = _fast_math32(L, y, ax)
     assert np.max(np.abs(sq2[big].astype(np.float64) - rs) / rs) <= 2.4e-7
+
+
+def test_fp32_atanh_third():
+    """The atanh polynomial of the FP32 deflection and potential (log(1 + t)/2 = atanh s for
+    |s| <= 1/3) against FP64 atanh, relative error, over |s| in [1e-30, 1/3]."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lenstool_hpc_b200 import build
+    build.build()
+    L = lt.load_library()
+    rng = np.random.default_rng(3)
+    m = np.concatenate([rng.uniform(0., 1. / 3., 200000), 10.0 ** rng.uniform(-30, np.log10(1. / 3.), 200000)])
+    s = (m * np.where(rng.random(m.size) < 0.5, -1., 1.)).astype(np.float32)
+    s = s[s != 0]
+    s = s[np.abs(s) <= np.float32(1. / 3.)]
+    th = _fast_math32(L, s, np.ones_like(s))[3]
+    ref = np.arctanh(s.astype(np.float64))
+    assert np.max(np.abs(th.astype(np.float64) - ref) / np.abs(ref)) <= 2.4e-7

@@ -90,7 +90,7 @@ def test_fp32c_sis_galaxies_and_kmap(ctx):
 
 
 def test_fp32c_host_outputs_and_potential(ctx):
-    """lens_maps in FP32C through host buffers; the potential stays FP64-exact."""
+    """lens_maps in FP32C through host buffers, the potential included."""
     cat = catalog.cluster_galaxy_catalog(2, 80, 7)
     g = catalog.Grid.square(100., 200)
     a = ctx.lens_maps(cat, g, precision="fp32c", dlsds=0.6)
@@ -98,7 +98,36 @@ def test_fp32c_host_outputs_and_potential(ctx):
     mask = np.isfinite(b["mu"]) & (np.abs(b["mu"]) <= 100)
     for k in ("kappa", "gamma1", "gamma2", "mu"):
         assert rel_errors(a[k], b[k], mask) <= TOL32, k
-    assert rel_errors(a["psi"], b["psi"], np.ones_like(mask)) <= 1e-6
+    e = rel_errors(a["psi"], b["psi"], np.ones_like(mask))
+    print("fp32c psi max rel err (82 halos):", e)
+    assert e <= TOL32
+
+
+@pytest.mark.parametrize("ptype", [81, 8, 5])
+def test_fp32c_potential_single_galaxies(ctx, ptype):
+    """The FP32 potential (deflection-based form) of lone galaxy-scale halos against the
+    LT_FP64 potential (the reference's pi05), over mass ellipticities 0.02-0.6 and core /
+    cut radii 0.01-0.8 / 5-50 arcsec (the FP32 class needs rc < 1), on a field reaching
+    150 arcsec from the centre; every pixel counts (the FP64 fallback regions included;
+    no pixel at a halo centre, where the reference's pi05 is 0/0)."""
+    import torch
+    cases = [(0.02, 0.1, 20.), (0.3, 0.05, 10.), (0.6, 0.01, 5.), (0.2, 0.8, 50.), (0.45, 0.3, 30.)]
+    g = catalog.Grid(-150., 150., -150., 150., 301, 301)
+    worst = 0.
+    for i, (em, rc, rcut) in enumerate(cases):
+        x0, y0 = 0.37 * (i + 1), -0.21 * (i + 1)
+        cat = catalog.make_catalog([ptype], [x0], [y0], [120.], [em], [0.4 + 0.5 * i], [rc], [rcut])
+        res = {}
+        for prec in ("fp32c", "fp64"):
+            psi = torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda")
+            ctx.potential_grid(cat, g, precision=prec, out=psi)
+            ctx.synchronize()
+            res[prec] = psi.cpu().numpy()
+        e = rel_errors(res["fp32c"], res["fp64"], np.ones((g.ny, g.nx), bool))
+        print(f"fp32c psi, lone type-{ptype} halo e_mass {em} rc {rc} rcut {rcut}: {e:.3e}")
+        worst = max(worst, e)
+        assert e <= TOL32, (ptype, em, rc, rcut, e)
+    print(f"fp32c psi max rel err, lone type-{ptype} halos: {worst}")
 
 
 @pytest.mark.parametrize("workload", ["grad_200h_1024", "maps_1000h_4096"])
@@ -117,5 +146,7 @@ def test_fp32c_deflection(ctx, workload):
         ctx.synchronize()
         res[prec] = (ax.cpu().numpy(), ay.cpu().numpy())
     mask = np.ones((g.ny, g.nx), bool)
+    errs = [rel_errors(res["fp32c"][i], res["fp64"][i], mask) for i in range(2)]
+    print(f"fp32c deflection max rel err {workload}: {errs}")
     for i in range(2):
-        assert rel_errors(res["fp32c"][i], res["fp64"][i], mask) <= TOL32, (workload, i)
+        assert errs[i] <= TOL32, (workload, i)

@@ -86,8 +86,46 @@ def test_grid_vs_oracle(ctx, oracle_lib, cluster_type, shape):
     psi = ctx.potential_grid(cat, g)
     opsi = oracle_lib.pot_grid(cat, g)
     assert max_rel_err(psi, opsi) <= TOL
-    # LT_FP64_FAST takes the potential through the N+- form (as accurate per term)
+    # LT_FP64_FAST takes the potential through the deflection (N+- form near its 0/0 points)
     assert max_rel_err(ctx.potential_grid(cat, g, precision="fp64fast"), opsi) <= TOL
+
+
+@pytest.mark.parametrize("ptype", [81, 8])
+def test_fp64fast_potential_near_removable_points(ctx, oracle_lib, ptype):
+    """LT_FP64_FAST takes the potential through the deflection (x . alpha plus one log per
+    radius), whose complex quotients are 0/0 at u = 0, v = 2 sqrt(e) r.  It keeps the N+-
+    form within 0.0316 rc of the core point and within 0.02 rcut of the cut point, and
+    (dPIE) takes log z_c - log z_t within 0.02 rcut of the core point.
+    Pixels on the points and at offsets from 1e-12 r up to beyond each switch, on both
+    sides of it, each relative to its own value, against pi05 in extended precision (the
+    oracle's x87 build): the reference's pi05 in FP64 is itself off by up to ~1e-12 of
+    the small potential close to a dPIE's centre."""
+    import oracle
+    x0, y0, ang = 3.3, -1.7, 0.7
+    rc, rcut = 0.4, 15.
+    cat = catalog.make_catalog([ptype], [x0], [y0], [180.], [0.3], [ang], [rc], [rcut])
+    e = float(cat.ellipticity_potential[0])
+    cs, sn = float(cat.anglecos[0]), float(cat.anglesin[0])
+    # (radius of the point, switch radii around it)
+    points = [(rc, [0.0316 * rc, 0.02 * rcut]), (rcut, [0.02 * rcut])] if ptype == 81 else [(rc, [0.0316 * rc])]
+    for r, edges in points:
+        offsets = [0., 1e-12 * r, 1e-8 * r, 1e-5 * r, 3e-3 * r] + [f * x for x in edges for f in (0.99, 1.01, 1.5)]
+        pts = []
+        for d in offsets:
+            for a in np.linspace(0., 2. * np.pi, 5, endpoint=False):
+                u = d * np.cos(a)
+                v = 2. * np.sqrt(e) * r + d * np.sin(a)
+                pts.append((x0 + u * cs - v * sn, y0 + u * sn + v * cs))
+        px = np.array([p[0] for p in pts])
+        py = np.array([p[1] for p in pts])
+        got = np.array([ctx.potential_grid(cat, catalog.Grid(x, x + 1., y, y + 1., 1, 1, dx=1., dy=1.),
+                                           precision="fp64fast")[0, 0] for x, y in zip(px, py)])
+        want = oracle.Oracle(oracle.ORACLE_LD_SO).pot_points(cat, px, py)
+        err = np.abs(got - want) / np.abs(want)
+        assert err.max() <= TOL, (ptype, r, err.max(), offsets[int(np.argmax(err)) // 5])
+        # and the FP64 oracle (pi05 as the reference rounds it) agrees to its own error
+        ref64 = oracle_lib.pot_points(cat, px, py)
+        assert np.max(np.abs(got - ref64) / np.abs(ref64)) <= 2e-12
 
 
 def test_every_map_kind_vs_oracle(ctx, oracle_lib):
