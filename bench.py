@@ -42,14 +42,21 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "maps_1000h_4096"
 METRIC = "halo x pixel evals/s (Hessian + potential, lens maps kappa/gamma1/gamma2/mu/psi)"
-# weighted flop census per pair (fixed convention: +,-,* = 1, fma = 2, div = sqrt = 4,
-# log = atan2 = 20): dPIE Hessian 182 (src/gradient2.cpp:92-167, :54-83) + dPIE potential
-# 760 (src/potential_GPU.cu:47-116 with src/lt_math_GPU.cuh)
+# weighted flop census per pair of the reference's own formulas (fixed convention:
+# +,-,* = 1, fma = 2, div = sqrt = 4, log = atan2 = 20): dPIE Hessian 182
+# (src/gradient2.cpp:92-167, :54-83) + dPIE potential 760 (src/potential_GPU.cu:47-116 with
+# src/lt_math_GPU.cuh).  The library's forms execute less than that (the potential goes
+# through the deflection), so this census is the roofline only of the modes measured below.
 FLOPS_PER_PAIR = 182 + 760
-# DRAM bytes (read + write) of one launch of the default step's dominant kernel
-# (grid32c_kernel<OP_HESS|OP_POT>, FP32C, 4096^2 x 1000 halos), from a single-pass ncu
-# capture of this bench's own launch: profiles/launches_lens_maps_fp32c_1000h_4096.md
-TRAFFIC_FP32C_LENS_4096 = 28883968 + 638935808
+# Work per pair that the default step's dominant kernel (grid32c_kernel<OP_HESS|OP_POT>,
+# FP32C, the 1000-halo catalogue) executes, from ncu's counters on the 1024^2 case of the
+# same catalogue (summary under profiles/): issued thread instructions (warp instructions
+# x 32 per pair) and FP32 flops (fadd + fmul + 2 ffma).  The kernel is issue-bound.
+INST_PER_PAIR_FP32C_LENS = 291.9
+FP32_FLOPS_PER_PAIR_FP32C_LENS = 246.5
+# DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
+# capture of this bench's own launch (summary under profiles/)
+TRAFFIC_FP32C_LENS_4096 = 27936768 + 634521088
 
 
 def _package():
@@ -654,7 +661,8 @@ def main():
             c2.release()
         torch.cuda.synchronize()
         e2e_value, _, _ = replicas.throughput(evals_step * args.steps, time.perf_counter() - t0, "cuda")
-        h2d = 192 * cat.n + 16 * cat.n
+        # FP64 records 256 B + FP32 records 160 B + index and type 8 B per halo, chunk tables
+        h2d = (256 + 160 + 8) * cat.n + 4 * 16 * ((cat.n + 63) // 64)
         d2h = len(names) * g.npix * 8
         e2e = {"value": e2e_value, "unit": "evals/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -667,6 +675,14 @@ def main():
         fpp = {"all": FLOPS_PER_PAIR, "hessian": 182, "potential": 760}[args.maps]
         achieved = g.npix * cat.n * fpp / per_launch / 1e12
         out_bytes = len(names) * g.npix * 8
+        pairs = g.npix * cat.n
+        issue = args.precision == "fp32c" and args.maps == "all"
+        if issue:
+            # the FMA-chain kernel issues one warp instruction per SMSP per cycle, the issue
+            # port's own rate: its flops / 2 is the peak of thread instructions per second
+            peak_inst = peak_tflops / 2 if peak_tflops else None
+            achieved_inst = pairs * INST_PER_PAIR_FP32C_LENS / per_launch / 1e12
+            fp32_tflops = pairs * FP32_FLOPS_PER_PAIR_FP32C_LENS / per_launch / 1e12
         cpu = None
         if not args.no_cpu_baseline:
             try:
@@ -685,19 +701,28 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "l2": "outputs 671 MB per step > 126 MB L2; catalogue 192 KB stays resident"},
             "gpu_launches": int(launches),
-            "roofline": {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                         "frac": achieved / peak_tflops if peak_tflops else None,
-                         "traffic": TRAFFIC_FP32C_LENS_4096 if (args.precision == "fp32c" and args.maps == "all"
-                                                                and not args.grid) else None,
-                         "traffic_algorithmic": out_bytes,
-                         "kernel": "lt::grid64_kernel<OP_HEX|OP_POT>" if args.precision == "fp64" else
-                         "lt::grid32c_kernel<OP_HESS|OP_POT>",
-                         "flops_per_pair": fpp, "flop_convention": "weighted census, FMA-equivalents",
-                         "peak_source": f"measured in-run: {pipe} FMA-chain kernel",
-                         "hbm_writeback_gbs": out_bytes / per_launch / 1e9,
-                         "hbm_peak_gbs": peaks.get("hbm_gbs")},
+            "roofline": ({"bound": "issue", "achieved": achieved_inst, "peak": peak_inst,
+                          "unit": "T thread-instructions/s",
+                          "frac": achieved_inst / peak_inst if peak_inst else None,
+                          "inst_per_pair": INST_PER_PAIR_FP32C_LENS,
+                          "fp32": {"flops_per_pair": FP32_FLOPS_PER_PAIR_FP32C_LENS, "achieved": fp32_tflops,
+                                   "peak": peak_tflops, "unit": "TFLOP/s",
+                                   "frac": fp32_tflops / peak_tflops if peak_tflops else None},
+                          "peak_source": "measured in-run: fp32 FMA-chain kernel (one warp instruction per "
+                                         "SMSP per cycle)",
+                          "time_basis": "whole step (pass 1 is ~95% of it)"} if issue else
+                         {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
+                          "frac": achieved / peak_tflops if peak_tflops else None,
+                          "flops_per_pair": fpp, "flop_convention": "weighted census of the reference's formulas",
+                          "peak_source": f"measured in-run: {pipe} FMA-chain kernel"}),
             "clocks": clocks.summary(),
         }
+        line["roofline"].update({
+            "traffic": TRAFFIC_FP32C_LENS_4096 if (issue and not args.grid) else None,
+            "traffic_algorithmic": out_bytes,
+            "kernel": "lt::grid64_kernel<OP_HEX|OP_POT>" if args.precision == "fp64" else
+                      "lt::grid32c_kernel<OP_HESS|OP_POT>",
+            "hbm_writeback_gbs": out_bytes / per_launch / 1e9, "hbm_peak_gbs": peaks.get("hbm_gbs")})
         if e2e:
             line["e2e"] = e2e
         if breakdown:
