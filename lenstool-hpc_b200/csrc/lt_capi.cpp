@@ -538,9 +538,7 @@ lt_status lt_lens_maps(lt_context *ctx, const lt_catalog *cat, const lt_grid *gr
 static bool sums_ok(int precision, int sums)
 {
     if (precision != LT_FP64 && precision != LT_FP32C && precision != LT_FP64_FAST) return false;
-    if (precision != LT_FP32C)
-        return sums == OP_GRAD || sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
-    return sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
+    return sums == OP_GRAD || sums == OP_HESS || sums == OP_POT || sums == (OP_HESS | OP_POT);
 }
 
 extern "C" {
