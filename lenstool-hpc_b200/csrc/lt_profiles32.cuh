@@ -216,20 +216,21 @@ __device__ __forceinline__ Log32 log32(const lt_rec32 &h, float u, float v)
     const float nr = h.cx1 * u;
     const float dci = h.s2rc - v;
     if (TYPE == 8) {
-        const float nci = h.s2 * o.wc - v * h.icx1;
-        /* z = N/D, A = |N|^2, B = |D|^2: log|z| = atanh((A - B)/(A + B)), where (with
-         * w_c^2 - rc^2 = rho^2) A - B = 2 v (4e v/(1-e)^2 - 2 sqrt(e) (w_c/cx1 - rc)) is taken
-         * without the cancellation of |N|^2 - |D|^2 near |z| = 1 (small e); arg z =
+        /* A PIEMD has no cut: its potential grows like b0 |x| with nothing to cancel the
+         * few-ulp error of the approximate instructions, so this branch (rare in the FP32
+         * class: galaxies are cut dPIEs) uses CUDA's accurate sqrtf, division, logf and
+         * atan2f.  z = N/D, A = |N|^2, B = |D|^2: log|z| = atanh((A - B)/(A + B)), where
+         * (with w_c^2 - rc^2 = rho^2) A - B = 2 v (4e v/(1-e)^2 - 2 sqrt(e) (w_c/cx1 - rc)) is
+         * taken without the cancellation of |N|^2 - |D|^2 near |z| = 1 (small e); arg z =
          * arg(N conj(D)), whose imaginary part u (2 sqrt(e) (w_c - cx1 rc) - v (1/cx1 - cx1))
          * avoids the same cancellation (1/cx1 - cx1 = 4e/(1-e^2)) */
+        o.wc = sqrtf(xc);
+        const float nci = h.s2 * o.wc - v * h.icx1;
         const float A = nr * nr + nci * nci, B = u * u + dci * dci;
         const float amb = 2.f * v * (h.e4 * h.cyi * v - h.s2 * fmaf(o.wc, h.icx1, -h.rc));
-        const float apb = A + B;
-        const float rs = frcp(apb);
-        const float s0 = amb * rs;
-        const float s = fmaf(rs, fmaf(-s0, apb, amb), s0);
-        o.lr = fabsf(s) <= (1.f / 3.f) ? fatanh_third(s) : 0.5f * __logf(A * frcp(B));
-        o.li = fatan2(u * (h.s2 * fmaf(-h.cx1, h.rc, o.wc) - v * (h.e4 * h.ome2)), nr * u + nci * dci);
+        const float s = amb / (A + B);
+        o.lr = fabsf(s) <= (1.f / 3.f) ? fatanh_third(s) : 0.5f * logf(A / B);
+        o.li = atan2f(u * (h.s2 * fmaf(-h.cx1, h.rc, o.wc) - v * (h.e4 * h.ome2)), nr * u + nci * dci);
         o.wt = 0.f;
         return o;
     }
@@ -303,6 +304,10 @@ __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v)
     if (TYPE == 5) return h.ppre * fsqrt(u * u * h.cx1 + v * v * h.icx1);
     const Log32 z = log32<TYPE>(h, u, v);
     const float ut = h.e4cxi * u * u;
+    if (TYPE == 8) { /* accurate operations, as in log32's PIEMD branch */
+        const float t = (z.rho2 / (z.wc + h.rc) * fmaf(h.om2, z.wc, h.ok3c) + ut) * h.i4rc2;
+        return h.ppre * ((u * z.li - v * z.lr) - h.s2 * h.rc * 0.5f * log1pf(t));
+    }
     float hs = h.rc * half_log1p_pos(tpot32(z.rho2, ut, z.wc, h.rc, h.ok3c, h.i4rc2, h.om2));
     if (TYPE == 81) hs -= h.rcut * half_log1p_pos(tpot32(z.rho2, ut, z.wt, h.rcut, h.ok3t, h.i4rcut2, h.om2));
     return h.ppre * ((u * z.li - v * z.lr) - h.s2 * hs);
