@@ -129,7 +129,7 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
             v[k] = ty * r.cs - tx * r.sn;
             const float rr = u[k] * u[k] + v[k] * v[k];
             const float dv = v[k] - r.singv;
-            near |= (rr < r.rnear2) | (u[k] * u[k] + dv * dv < r.sing_r2) | (rr < r.core_r2);
+            near |= (rr < r.rnear2) | (u[k] * u[k] + dv * dv < r.sing_r2);
         }
         /* the FP64 fallback regions (an FP64 proxy record has rnear2 = +inf: every pixel) */
         if (__any_sync(0xffffffffu, near)) {

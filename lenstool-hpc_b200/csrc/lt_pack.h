@@ -213,7 +213,9 @@ LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     o.singv = f32(mul(mul(2., sr), sqe));
     const double srad = mul(add(kSingFrac, mul(kSingEps, e)), sr);
     o.sing_r2 = f32(mul(srad, srad));
-    o.core_r2 = f32(mul(mul(kCoreFrac, r.rc), mul(kCoreFrac, r.rc)));
+    const double core_r2 = mul(mul(kCoreFrac, r.rc), mul(kCoreFrac, r.rc));
+    /* one radius for both round regions: the near field and the core */
+    if (core_r2 > mul(near_r, near_r)) o.rnear2 = f32(core_r2);
 }
 
 } // namespace pk

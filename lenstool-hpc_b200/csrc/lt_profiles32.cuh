@@ -34,7 +34,9 @@ struct alignas(16) lt_rec32 {
     float cyi, ome2, e4, kpre;    /* 1/(1-e)^2, 1/(1-e^2), 4e, kappa prefactor               */
     float gpre, rc, rcut, drs;    /* gamma prefactor, rc, rcut, rc - rcut                    */
     float dr2, rc2, rcut2, w;     /* rc^2 - rcut^2, rc^2, rcut^2, Kmap weight                */
-    float rnear2, singv, sing_r2, core_r2; /* FP64 fallback regions (squared radii)          */
+    float rnear2, singv, sing_r2, pad2;    /* FP64 fallback regions: squared radius of the near
+                                              field or core (larger of the two), the cut
+                                              radius's singular point and its squared radius */
     float cpi, s2rc, s2rcut, ok3c; /* cx1 + 1/cx1, 2 sqrt(e) rc, 2 sqrt(e) rcut, (1-e)(3+e) rc */
     float om2, e4cxi, ppre, i4rc2; /* potential: (1-e)^2, 4e/(1+e)^2, prefactor, 1/(4 rc^2)    */
     int32_t type, idx64;
@@ -251,9 +253,7 @@ __device__ __forceinline__ Log32 log32(const lt_rec32 &h, float u, float v)
     const float B = denr * denr + deni * deni;
     const float amb = fmaf(2.f, c, numr * numr + numi * numi); /* A - B */
     const float apb = fmaf(2.f, B, amb);                       /* A + B */
-    const float rs = frcp(apb);
-    const float s0 = amb * rs;
-    const float s = fmaf(rs, fmaf(-s0, apb, amb), s0); /* (A - B)/(A + B), one correction step */
+    const float s = amb * frcp(apb); /* (A - B)/(A + B) */
     o.lr = fabsf(s) <= (1.f / 3.f) ? fatanh_third(s) : 0.5f * __logf((B + amb) * frcp(B));
     o.li = fatan2(d, B + c);
     return o;
