@@ -308,8 +308,10 @@ __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v)
         const float t = (z.rho2 / (z.wc + h.rc) * fmaf(h.om2, z.wc, h.ok3c) + ut) * h.i4rc2;
         return h.ppre * ((u * z.li - v * z.lr) - h.s2 * h.rc * 0.5f * log1pf(t));
     }
-    float hs = h.rc * half_log1p_pos(tpot32(z.rho2, ut, z.wc, h.rc, h.ok3c, h.i4rc2, h.om2));
-    if (TYPE == 81) hs -= h.rcut * half_log1p_pos(tpot32(z.rho2, ut, z.wt, h.rcut, h.ok3t, h.i4rcut2, h.om2));
+    /* core term: outside the FP64 regions (3 rc and more from the centre) t_c > 0.44, where
+     * __logf(1 + t) is within 1.8e-7 absolute, on a term that carries rc << rcut */
+    float hs = h.rc * 0.5f * __logf(1.f + tpot32(z.rho2, ut, z.wc, h.rc, h.ok3c, h.i4rc2, h.om2));
+    hs -= h.rcut * half_log1p_pos(tpot32(z.rho2, ut, z.wt, h.rcut, h.ok3t, h.i4rcut2, h.om2));
     return h.ppre * ((u * z.li - v * z.lr) - h.s2 * hs);
 }
 
