@@ -52,11 +52,11 @@ FLOPS_PER_PAIR = 182 + 760
 # FP32C, the 1000-halo catalogue) executes, from ncu's counters on the 1024^2 case of the
 # same catalogue (summary under profiles/): issued thread instructions (warp instructions
 # x 32 per pair) and FP32 flops (fadd + fmul + 2 ffma).  The kernel is issue-bound.
-INST_PER_PAIR_FP32C_LENS = 291.9
-FP32_FLOPS_PER_PAIR_FP32C_LENS = 246.5
+INST_PER_PAIR_FP32C_LENS = 278.7
+FP32_FLOPS_PER_PAIR_FP32C_LENS = 241.1
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
-TRAFFIC_FP32C_LENS_4096 = 27936768 + 634521088
+TRAFFIC_FP32C_LENS_4096 = 19494912 + 631581696
 
 
 def _package():
@@ -339,7 +339,7 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
     return res
 
 
-def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=12, seed=20261203 + 4):
+def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=None, seed=20261203 + 4):
     """Serving workload: Poisson arrivals at `rate` req/s of requests drawn uniformly from
     {deflection map, kappa/gamma1/gamma2/mu maps, chi2}, grids U{512^2, 1024^2, 2048^2,
     4096^2}.  Map requests use catalogues with log-uniform(50, 5000) halos (1% cluster-scale)
@@ -422,8 +422,9 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=12, se
     r70 = 0.7 * sat["requests_per_s"]
     res["at_70pct_capacity"] = dict(run(arrivals * rate / r70), rate_per_s=r70)
     # one plain FP64 call per request (host outputs / host chi2, the reference's calling
-    # pattern), a sample scaled to all requests by halo x pixel evaluations of their grids
-    idx = list(range(plain_sample))
+    # pattern): every request by default (a smaller sample is scaled to all requests by the
+    # halo x pixel evaluations of their grids)
+    idx = list(range(plain_sample or n_requests))
     t0 = time.perf_counter()
     for i in idx:
         k, n, c = reqs[i]
@@ -451,8 +452,8 @@ def bench_chi2(ctx, n_models=64, n=2048, nsys=40, seed=20261203 + 3, cpu=True):
     catalogue against 40 multiple-image systems with 3-5 images each, generated by
     forward ray-shooting of seeded sources through the true model (delensing on a 2048^2
     grid) plus 0.05" Gaussian noise; per model a 2048^2 deflection grid, barycentric
-    delensing and the FP64 chi2 (lt_chi2_batch).  A sample of n_models models is timed
-    (the 4096-model batch takes 4096 / models_per_s)."""
+    delensing and the FP64 chi2 (lt_chi2_batch).  A sample of n_models models is timed,
+    each leg as the median of three runs (the 4096-model batch takes 4096 / models_per_s)."""
     lt = _package()
     from lenstool_hpc_b200 import catalog
     from lenstool_hpc_b200.images import generate_systems
@@ -466,10 +467,17 @@ def bench_chi2(ctx, n_models=64, n=2048, nsys=40, seed=20261203 + 3, cpu=True):
                                centre=(base.position_x[ic], base.position_y[ic]), source_radius=10.)
     rng = np.random.Generator(np.random.PCG64(seed + 1))
     models = [ctx.upload(catalog.perturb_catalog(base, rng)) for _ in range(n_models)]
-    ctx.chi2(models[:2], frame, n, systems)  # warm-up
-    t0 = time.perf_counter()
-    chi, found = ctx.chi2(models, frame, n, systems)
-    dt = time.perf_counter() - t0
+    def timed(precision, runs=3):
+        """median wall time of `runs` calls over all models (host-side work included)"""
+        ctx.chi2(models[:2], frame, n, systems, precision=precision)  # warm-up
+        ts = []
+        for _ in range(runs):
+            t0 = time.perf_counter()
+            out = ctx.chi2(models, frame, n, systems, precision=precision)
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), out
+
+    dt, (chi, found) = timed("fp64")
     true_chi, _ = ctx.chi2(dbase, frame, n, systems)
     res = {"workload": f"chi2_batch: {n_models} of 4096 perturbed models x {base.n} halos, {nsys} systems "
                        f"({systems.nimages} images), {n}^2 delensing grid, FP64",
@@ -477,10 +485,7 @@ def bench_chi2(ctx, n_models=64, n=2048, nsys=40, seed=20261203 + 3, cpu=True):
            "seconds_for_4096_models": 4096 * dt / n_models, "deflection_evals_per_s": n_models * n * n * base.n / dt,
            "chi2_true_model": true_chi, "chi2_median_perturbed": float(np.median(chi))}
     # the deflection grid in LT_FP32C, delensing and chi2 in FP64
-    ctx.chi2(models[:2], frame, n, systems, precision="fp32c")
-    t0 = time.perf_counter()
-    chi32, found32 = ctx.chi2(models, frame, n, systems, precision="fp32c")
-    dt32 = time.perf_counter() - t0
+    dt32, (chi32, found32) = timed("fp32c")
     res["fp32c_deflections"] = {
         "models_per_s": n_models / dt32, "ms_per_model": 1e3 * dt32 / n_models,
         "same_images_found": bool(np.array_equal(found32, found)),
