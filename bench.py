@@ -520,7 +520,7 @@ def main():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="--impl reference: skip timing the reference's GPU kernels beside its CPU code")
     ap.add_argument("--grid", type=int, default=0, help="smaller square grid (profiling cases)")
-    ap.add_argument("--maps", default="all", choices=["all", "hessian", "potential"],
+    ap.add_argument("--maps", default="all", choices=["all", "hessian", "potential", "deflection"],
                     help="all = kappa/gamma1/gamma2/mu/psi (the workload); the others time one sum")
     ap.add_argument("--breakdown", action="store_true", help="also time the Hessian-only and potential-only passes")
     ap.add_argument("--no-fp64-compare", action="store_true", help="skip timing LT_FP64 on the same workload")
@@ -576,12 +576,19 @@ def main():
     dcat = ctx.upload(cat)
     stream = torch.cuda.Stream()
     names = {"all": ("kappa", "gamma1", "gamma2", "mu", "psi"), "hessian": ("kappa", "gamma1", "gamma2", "mu"),
-             "potential": ("psi",)}[args.maps]
+             "potential": ("psi",), "deflection": ("deflection_x", "deflection_y")}[args.maps]
     sums_per_pair = (2 if args.maps == "all" else 1)
     outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in names}
 
+    def maps_call(c, prec, o, stream=None, which=names):
+        """the timed call: the lens maps in one fused pass, or the deflection grid"""
+        if args.maps == "deflection":
+            ctx.gradient_grid(c, g, precision=prec, out=(o["deflection_x"], o["deflection_y"]), stream=stream)
+        else:
+            ctx.lens_maps(c, g, precision=prec, dlsds=D, out=o, stream=stream, which=which)
+
     def step(which=names, o=outs):
-        ctx.lens_maps(dcat, g, precision=args.precision, dlsds=D, out=o, stream=stream, which=which)
+        maps_call(dcat, args.precision, o, stream, which)
 
     for _ in range(warmup):
         step()
@@ -633,11 +640,11 @@ def main():
     fp64_cmp = None
     if rank == 0 and args.precision != "fp64" and not args.no_fp64_compare:
         def time_precision(prec, k=2):
-            ctx.lens_maps(dcat, g, precision=prec, dlsds=D, out=outs, stream=stream, which=names)
+            maps_call(dcat, prec, outs, stream)
             f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             f0.record(stream)
             for _ in range(k):
-                ctx.lens_maps(dcat, g, precision=prec, dlsds=D, out=outs, stream=stream, which=names)
+                maps_call(dcat, prec, outs, stream)
             f1.record(stream)
             ctx.synchronize(stream)
             return f0.elapsed_time(f1) / 1e3 / k
@@ -656,13 +663,13 @@ def main():
         hnp = {k: v.numpy() for k, v in host.items()}
         for _ in range(1):
             c2 = ctx.upload(cat)
-            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp, which=names)
+            maps_call(c2, args.precision, hnp)
             c2.release()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
             c2 = ctx.upload(cat)
-            ctx.lens_maps(c2, g, precision=args.precision, dlsds=D, out=hnp, which=names)
+            maps_call(c2, args.precision, hnp)
             c2.release()
         torch.cuda.synchronize()
         e2e_value, _, _ = replicas.throughput(evals_step * args.steps, time.perf_counter() - t0, "cuda")
@@ -677,8 +684,8 @@ def main():
         peaks = measured_peaks()
         pipe = "fp32" if args.precision == "fp32c" else "fp64"
         peak_tflops = fma_peak_tflops(pipe)
-        fpp = {"all": FLOPS_PER_PAIR, "hessian": 182, "potential": 760}[args.maps]
-        achieved = g.npix * cat.n * fpp / per_launch / 1e12
+        fpp = {"all": FLOPS_PER_PAIR, "hessian": 182, "potential": 760}.get(args.maps)  # no census: deflection
+        achieved = g.npix * cat.n * fpp / per_launch / 1e12 if fpp else None
         out_bytes = len(names) * g.npix * 8
         pairs = g.npix * cat.n
         issue = args.precision == "fp32c" and args.maps == "all"
@@ -717,7 +724,7 @@ def main():
                                          "SMSP per cycle)",
                           "time_basis": "whole step (pass 1 is ~95% of it)"} if issue else
                          {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
-                          "frac": achieved / peak_tflops if peak_tflops else None,
+                          "frac": achieved / peak_tflops if (peak_tflops and achieved) else None,
                           "flops_per_pair": fpp, "flop_convention": "weighted census of the reference's formulas",
                           "peak_source": f"measured in-run: {pipe} FMA-chain kernel"}),
             "clocks": clocks.summary(),
@@ -725,8 +732,9 @@ def main():
         line["roofline"].update({
             "traffic": TRAFFIC_FP32C_LENS_4096 if (issue and not args.grid) else None,
             "traffic_algorithmic": out_bytes,
-            "kernel": "lt::grid64_kernel<OP_HEX|OP_POT>" if args.precision == "fp64" else
-                      "lt::grid32c_kernel<OP_HESS|OP_POT>",
+            "kernel": ("lt::grid64_kernel" if args.precision in ("fp64", "fp64fast") else "lt::grid32c_kernel") +
+                      {"all": "<OP_HESS|OP_POT>", "hessian": "<OP_HESS>", "potential": "<OP_POT>",
+                       "deflection": "<OP_GRAD>"}[args.maps],
             "hbm_writeback_gbs": out_bytes / per_launch / 1e9, "hbm_peak_gbs": peaks.get("hbm_gbs")})
         if e2e:
             line["e2e"] = e2e
