@@ -433,7 +433,9 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
         const int xop = ((op & OP_HESS) ? ((op & ~OP_HESS) | OP_HEX) : op) | ((op & OP_POT) ? OP_PEX : 0);
         err = launch_grid64_tiled(xop, a, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
     } else if (precision == LT_FP64_FAST) {
-        err = launch_grid64_tiled(op, a, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][op & 7]);
+        /* the dPIE deflection as log(1 + eps) (a deflection-only call: no kernel combines it) */
+        const int fop = op == OP_GRAD ? (OP_GRAD | OP_GFX) : op;
+        err = launch_grid64_tiled(fop, a, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][op & 7]);
     } else {
         err = launch_fp32c(ctx, cat, op, a, s);
     }

@@ -31,7 +31,8 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
         double w = kmap ? r.w : 1.0;
 #pragma unroll
         for (int k = 0; k < P; k++) {
-            if (OP & OP_GRAD) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
+            if ((OP & OP_GRAD) && (OP & OP_GFX)) grad_pair_fast<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
+            if ((OP & OP_GRAD) && !(OP & OP_GFX)) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
             if (OP & OP_HESS) {
                 Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
                 hess_pair<TYPE>(r, px[k], py, w, hh);

@@ -18,8 +18,10 @@ enum {
 /* which sums a kernel evaluates; OP_HEX is the Hessian with the reference's rounding
  * sequence (LT_FP64), OP_HESS the reformulated one (LT_FP64_FAST and the FP32C path);
  * OP_PEX with OP_POT takes the potential through the reference's pi05 formula (LT_FP64),
- * OP_POT alone through the cancellation-free N+- form (LT_FP64_FAST, FP32C's FP64 halos) */
-enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4, OP_HEX = 8, OP_PEX = 16 };
+ * OP_POT alone through the deflection (LT_FP64_FAST, FP32C's FP64 halos); OP_GFX with
+ * OP_GRAD takes the dPIE deflection as log(1 + eps) (LT_FP64_FAST), OP_GRAD alone in the
+ * reference's two-logarithm form (LT_FP64, the queue's exact tiles, the chi2 points) */
+enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4, OP_HEX = 8, OP_PEX = 16, OP_GFX = 32 };
 
 /* chunk.pad bits: FP32 records (FP32C list), last chunk of a run */
 enum { CHUNK_FP32 = 1, CHUNK_RUN_END = 2 };

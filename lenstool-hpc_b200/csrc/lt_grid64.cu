@@ -187,6 +187,7 @@ int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool 
     }
     switch (op) {
     case OP_GRAD: return launch_shape<OP_GRAD>(shape, args, num_sms, s);
+    case OP_GRAD | OP_GFX: return launch_shape<OP_GRAD | OP_GFX>(shape, args, num_sms, s);
     case OP_HESS: return launch_shape<OP_HESS>(shape, args, num_sms, s);
     case OP_POT: return launch_shape<OP_POT>(shape, args, num_sms, s);
     case OP_HESS | OP_POT: return launch_shape<OP_HESS | OP_POT>(shape, args, num_sms, s);

@@ -377,6 +377,30 @@ __device__ __forceinline__ double pot64_defl(const lt_rec64 &h, double u, double
 constexpr double kSingCut64 = 4e-4;  /* x rcut^2 */
 constexpr double kSingCore64 = 1e-3; /* x rc^2 */
 
+/* The deflection of LT_FP64_FAST: for a dPIE pair away from its two 0/0 points, the
+ * cancellation-free log(1 + eps) of log64 (1 log1p + 1 atan2, in place of the reference's
+ * 2 log + 2 atan2); within 0.02 rcut of either point, and for PIEMD and SIS, the reference's
+ * form of grad_pair.  alpha = pref (arg, -log| |) of z_c/z_t in the halo frame, as grad_pair. */
+template <int TYPE>
+__device__ __forceinline__ void grad_pair_fast(const lt_rec64 &h, double px, double py, double &gx, double &gy)
+{
+    if (TYPE != 81) {
+        grad_pair<TYPE>(h, px, py, gx, gy);
+        return;
+    }
+    Frame64 f = to_frame(h, px, py);
+    const double u = f.u, v = f.v, uu = u * u;
+    const double dvc = v - h.tsr_c, dvt = v - h.tsr_t;
+    if ((uu + dvc * dvc < kSingCut64 * h.rcut2) | (uu + dvt * dvt < kSingCut64 * h.rcut2)) {
+        grad_pair<TYPE>(h, px, py, gx, gy);
+        return;
+    }
+    const Log64 z = log64<81>(h, u, v, uu, uu * h.cxro_inv + v * v * h.cyro_inv, false);
+    const double re = h.pref_g * z.li, im = -h.pref_g * z.lr;
+    gx += re * h.cs - im * h.sn;
+    gy += im * h.cs + re * h.sn;
+}
+
 template <int TYPE>
 __device__ __forceinline__ void pot_pair_fast(const lt_rec64 &h, double px, double py, double &psi)
 {

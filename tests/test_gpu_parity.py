@@ -75,6 +75,9 @@ def test_grid_vs_oracle(ctx, oracle_lib, cluster_type, shape):
     ax, ay = ctx.gradient_grid(cat, g)
     ox, oy = oracle_lib.grad_grid(cat, g)
     assert max_rel_err(ax, ox) <= TOL and max_rel_err(ay, oy) <= TOL
+    # LT_FP64_FAST: the dPIE deflection as log(1 + eps) away from its 0/0 points
+    fx, fy = ctx.gradient_grid(cat, g, precision="fp64fast")
+    assert max_rel_err(fx, ox) <= TOL and max_rel_err(fy, oy) <= TOL
     h = ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c", "hess_d"])
     oh = oracle_lib.hess_grid(cat, g)
     for k, name in enumerate(["hess_a", "hess_b", "hess_c", "hess_d"]):
@@ -126,6 +129,23 @@ def test_fp64fast_potential_near_removable_points(ctx, oracle_lib, ptype):
         # and the FP64 oracle (pi05 as the reference rounds it) agrees to its own error
         ref64 = oracle_lib.pot_points(cat, px, py)
         assert np.max(np.abs(got - ref64) / np.abs(ref64)) <= 2e-12
+
+
+def test_fp64fast_deflection_workload(ctx):
+    """LT_FP64_FAST deflection (log(1 + eps) for dPIE pairs, the reference's form within
+    0.02 rcut of the 0/0 points) against LT_FP64 on the 1000-halo workload field at 768^2."""
+    import torch
+    cat, g0 = catalog.workload("maps_1000h_4096")
+    g = catalog.Grid(g0.xmin, g0.xmax, g0.ymin, g0.ymax, 768, 768)
+    res = {}
+    for prec in ("fp64", "fp64fast"):
+        ax = torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda")
+        ay = torch.empty_like(ax)
+        ctx.gradient_grid(cat, g, precision=prec, out=(ax, ay))
+        ctx.synchronize()
+        res[prec] = (ax.cpu().numpy(), ay.cpu().numpy())
+    for i in range(2):
+        assert max_rel_err(res["fp64fast"][i], res["fp64"][i]) <= TOL, i
 
 
 def test_every_map_kind_vs_oracle(ctx, oracle_lib):
