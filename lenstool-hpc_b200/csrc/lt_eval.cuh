@@ -108,7 +108,7 @@ __device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, co
                 acc.hxy[k] = hh.xy;
             }
             if (OP & OP_POT) pot_pair_fast<TYPE>(r, px[k], py, acc.psi[k]);
-            if (OP & OP_GRAD) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
+            if (OP & OP_GRAD) grad_pair_fast<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
         }
     }
 }
@@ -145,7 +145,7 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
                     acc.hyy[k] = hh.yy;
                     acc.hxy[k] = hh.xy;
                 }
-                if (OP & OP_GRAD) grad_pair<TYPE>(r64, px[k], py, acc.gx[k], acc.gy[k]);
+                if (OP & OP_GRAD) grad_pair_fast<TYPE>(r64, px[k], py, acc.gx[k], acc.gy[k]);
                 if (OP & OP_POT) pot_pair_fast<TYPE>(r64, px[k], py, acc.psi[k]);
             }
         } else {

@@ -19,8 +19,9 @@ enum {
  * sequence (LT_FP64), OP_HESS the reformulated one (LT_FP64_FAST and the FP32C path);
  * OP_PEX with OP_POT takes the potential through the reference's pi05 formula (LT_FP64),
  * OP_POT alone through the deflection (LT_FP64_FAST, FP32C's FP64 halos); OP_GFX with
- * OP_GRAD takes the dPIE deflection as log(1 + eps) (LT_FP64_FAST), OP_GRAD alone in the
- * reference's two-logarithm form (LT_FP64, the queue's exact tiles, the chi2 points) */
+ * OP_GRAD takes the dPIE deflection as log(1 + eps) (LT_FP64_FAST; FP32C's FP64 terms
+ * always do), OP_GRAD alone in the reference's two-logarithm form (LT_FP64, the queue's
+ * exact tiles, the chi2 points) */
 enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4, OP_HEX = 8, OP_PEX = 16, OP_GFX = 32 };
 
 /* chunk.pad bits: FP32 records (FP32C list), last chunk of a run */
