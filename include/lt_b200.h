@@ -52,7 +52,9 @@ typedef enum {
  *          sequence (bit-identical to the reference CPU path), deflection and potential
  *          agree to <= 1e-12.
  * LT_FP32C: FP32 bulk with compensated accumulation and FP64 where FP32 loses digits.
- * LT_FP64_FAST: FP64 with reciprocals, FMA and shared sub-expressions; within 2e-12 of
+ * LT_FP64_FAST: FP64 with reciprocals, FMA and shared sub-expressions, the dPIE deflection
+ *          as log(z_c/z_t) taken without cancellation and the potential through the
+ *          deflection (x . alpha plus one logarithm per core radius); within 2e-12 of
  *          the reference except at the formula's ill-conditioned pixels (within ~1e-3"
  *          of each halo's removable singular points), where it departs by up to ~1e-11. */
 typedef enum { LT_FP64 = 0, LT_FP32C = 1, LT_FP64_FAST = 2 } lt_precision;
