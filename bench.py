@@ -51,7 +51,12 @@ FLOPS_PER_PAIR = 182 + 760
 # Work per pair that the default step's dominant kernel (grid32c_kernel<OP_HESS|OP_POT>,
 # FP32C, the 1000-halo catalogue) executes, from ncu's counters on the 1024^2 case of the
 # same catalogue (summary under profiles/): issued thread instructions (warp instructions
-# x 32 per pair) and FP32 flops (fadd + fmul + 2 ffma).  The kernel is issue-bound.
+# x 32 per pair) and FP32 flops (fadd + fmul + 2 ffma).  The kernel is issue-bound.  The
+# figures hold for the build whose KERNEL_SOURCES hash to INST_SOURCES_SHA; the bench line
+# says whether the timed build is that one.
+KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
+                  "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
+INST_SOURCES_SHA = "pending"
 INST_PER_PAIR_FP32C_LENS = 278.7
 FP32_FLOPS_PER_PAIR_FP32C_LENS = 241.1
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
@@ -139,37 +144,56 @@ def measured_peaks():
 
 
 def reference_cpu(steps, warmup, rows=None):
-    """Reference CPU code on a band of rows of the workload; returns (evals/s, info)."""
+    """Reference CPU code on bands of rows of the workload; returns (evals/s, info).
+
+    gradient2_grid_CPU spreads its rows over the OpenMP threads (`#pragma omp for` over
+    rows, src/grid_gradient2_CPU.cpp:68-70), so every band has as many rows as there are
+    threads (each thread one row of 4096 pixels); the potential kernel runs over the same
+    pixels with a dynamic schedule.  Two bands, at a quarter and three quarters of the
+    field's height, so that the sample is not one strip through the centre."""
     import oracle
     lt = _package()
     from lenstool_hpc_b200 import catalog
     ref = oracle.RefLib()
     cat, g = catalog.workload(WORKLOAD)
     threads = os.cpu_count()
-    rows = rows or max(1, min(64, threads // 4))
-    band = catalog.Grid(g.xmin, g.xmax, g.ymin, g.ymax, g.nx, rows, 0, g.ny // 2, dx=g.dx, dy=g.dy)
-    times = []
+    rows = rows or threads
+    bands = [catalog.Grid(g.xmin, g.xmax, g.ymin, g.ymax, g.nx, rows, 0, j0, dx=g.dx, dy=g.dy)
+             for j0 in (g.ny // 4 - rows // 2, 3 * g.ny // 4 - rows // 2)]
+    times, th, tp = [], [], []
     for it in range(warmup + steps):
-        t0 = time.perf_counter()
-        ref.hess_grid(cat, band)
-        px, py = band.coords()
-        ref.pot81_points(cat, px, py)
-        dt = time.perf_counter() - t0
+        h = p = 0.
+        for band in bands:
+            t0 = time.perf_counter()
+            ref.hess_grid(cat, band)
+            t1 = time.perf_counter()
+            px, py = band.coords()
+            ref.pot81_points(cat, px, py)
+            h += t1 - t0
+            p += time.perf_counter() - t1
         if it >= warmup:
-            times.append(dt)
-    evals = 2 * band.npix * cat.n
+            times.append(h + p)
+            th.append(h)
+            tp.append(p)
+    npix = sum(b.npix for b in bands)
+    evals = 2 * npix * cat.n
     v = evals / float(np.mean(times))
-    sample = (f"{rows} rows x {g.nx} px x {cat.n} halos of the workload (gradient2_grid_CPU + reference potential "
-              f"kernel on the host), {threads} OpenMP threads")
+    sample = (f"{len(bands)} bands of {rows} rows x {g.nx} px x {cat.n} halos of the workload (gradient2_grid_CPU "
+              f"+ the reference potential kernel on the host), {threads} OpenMP threads, one row per thread")
     return v, {"value": v, "unit": "evals/s", "cores": threads, "kind": "reference", "sample": sample,
+               "threads_busy": {"hessian": min(threads, rows), "potential": threads},
+               "hessian_evals_per_s": npix * cat.n / float(np.mean(th)),
+               "potential_evals_per_s": npix * cat.n / float(np.mean(tp)),
                "seconds_per_sample": float(np.mean(times))}
 
 
 def reference_gpu(reps=1, band_rows=32):
     """The reference's own GPU kernels (src/gradient2_GPU.cu, src/potential_GPU.cu, built
-    for sm_100a from its sources, type_t = double and float) on the full workload, one
-    Hessian and one potential launch per step as its wrappers make them (32 x 16 threads,
-    one pixel per thread); evals counted as for `value`.  Each build's error is measured
+    for sm_100a from its sources) on the full workload, one Hessian and one potential
+    launch per step as its wrappers make them (32 x 16 threads, one pixel per thread);
+    evals counted as for `value`.  Builds: fp64_stock (the flags of the reference's
+    default build: -O3 -use_fast_math, type_t = double), fp32_stock (the same with
+    type_t = float), and fp64 / fp32 with -O3 alone.  Each build's error is measured
     against the reference CPU FP64 code on a band of rows."""
     import oracle
     from lenstool_hpc_b200 import catalog
@@ -178,7 +202,7 @@ def reference_gpu(reps=1, band_rows=32):
     bgrid = catalog.Grid(g.xmin, g.xmax, g.ymin + (g.ny // 2) * g.dy, g.ymax, g.nx, band_rows, dx=g.dx, dy=g.dy)
     cpu_h = cpu_p = None
     out = {"workload": WORKLOAD, "launch": "reference kernels, 32x16 threads, one pixel per thread"}
-    for build in ("fp64", "fp32"):
+    for build in ("fp64_stock", "fp32_stock", "fp64", "fp32"):
         try:
             lib = oracle.RefGpuLib(build)
             th, _ = lib.grid("hessian", cat, g, reps=reps, want=False)
@@ -235,6 +259,12 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
     rows_dev = torch.tensor(rows, device="cuda")
     outs = [{k: torch.empty((int(n), int(n)), dtype=torch.float64, device="cuda") for k in kinds} for n in sizes]
     reqs = [lt.Request(c, grids[int(n)], o, dlsds=D) for c, n, o in zip(cats, sizes, outs)]
+    tune = None
+    if precision == "fp32c":
+        # the Hessian kernel configuration tuned on the model's catalogue (the batch takes
+        # its pixels per thread and CTAs per SM)
+        ppt, cps, tms = ctx.autotune(cats[0], precision, "hessian", grid_n=512)
+        tune = dict(ctx.kernel_config(precision, "hessian"), ms_at_512=tms)
     batch = ctx.batch(reqs, precision=precision)
     evals = float(sum(int(n) * int(n) for n in sizes)) * base.n
     stream = torch.cuda.Stream()
@@ -256,7 +286,8 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
                        f"mu+kappa", "precision": precision, "maps_per_s": 2 * n_sets / dt, "sets_per_s": n_sets / dt,
            "evals_per_s": evals / dt, "ms_per_step": dt * 1e3, "gpu_launches_per_step": launches / steps,
            "evals_per_step": evals, "l2": f"outputs {2 * 8 * evals / base.n / 1e9:.1f} GB per step > L2",
-           "step": "lt_bayes_apply of the rows (HBM) + one lt_batch graph"}
+           "step": "lt_bayes_apply of the rows (HBM) + one lt_batch graph",
+           "shape": dict(batch.config(), autotuned=tune)}
     # the sets as host catalogues (the reference's host-side row update), for the plain loop
     sets = [bayes.catalog_from_state(model, bayes.reference_state(model, (), cols, rows[i]))
             for i in range(plain_sample)]
@@ -421,27 +452,32 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=None, 
     # a second pass at 70% of the measured capacity (the queue does not build up)
     r70 = 0.7 * sat["requests_per_s"]
     res["at_70pct_capacity"] = dict(run(arrivals * rate / r70), rate_per_s=r70)
-    # one plain FP64 call per request (host outputs / host chi2, the reference's calling
-    # pattern): every request by default (a smaller sample is scaled to all requests by the
-    # halo x pixel evaluations of their grids)
+    # one plain call per request (host outputs / host chi2, the reference's calling
+    # pattern), in FP64 and in the server's own precision: every request by default (a
+    # smaller sample is scaled to all requests by the halo x pixel evaluations of their grids)
     idx = list(range(plain_sample or n_requests))
-    t0 = time.perf_counter()
-    for i in idx:
-        k, n, c = reqs[i]
-        g = catalog.Grid.square(100., n)
-        if k == 0:
-            ctx.gradient_grid(dcats[c], g, precision="fp64", scale=D)
-        elif k == 1:
-            ctx.hessian_maps(dcats[c], g, list(kinds_of[1]), precision="fp64", dlsds=D)
-        else:
-            ctx.chi2(models[c], frame, n, systems)
-    t = time.perf_counter() - t0
     sample_evals = float(sum(reqs[i][1] ** 2 * halos(reqs[i][0], reqs[i][2]) for i in idx))
-    t_all = t * evals / sample_evals
-    res["one_request_per_call_fp64"] = {"requests_per_s": len(reqs) / t_all, "maps_per_s": nmaps / t_all,
-                                        "sample_requests": len(idx), "sample_s": t}
+    for prec in dict.fromkeys(("fp64", precision)):
+        t0 = time.perf_counter()
+        for i in idx:
+            k, n, c = reqs[i]
+            g = catalog.Grid.square(100., n)
+            if k == 0:
+                ctx.gradient_grid(dcats[c], g, precision=prec, scale=D)
+            elif k == 1:
+                ctx.hessian_maps(dcats[c], g, list(kinds_of[1]), precision=prec, dlsds=D)
+            else:
+                ctx.chi2(models[c], frame, n, systems, precision=prec)
+        t = time.perf_counter() - t0
+        t_all = t * evals / sample_evals
+        key = "one_request_per_call_" + ("fp64" if prec == "fp64" else "same_precision")
+        res[key] = {"precision": prec, "requests_per_s": len(reqs) / t_all, "maps_per_s": nmaps / t_all,
+                    "sample_requests": len(idx), "sample_s": t}
     res["speedup_vs_one_request_per_call_fp64"] = (sat["requests_per_s"] /
                                                    res["one_request_per_call_fp64"]["requests_per_s"])
+    if "one_request_per_call_same_precision" in res:
+        res["speedup_vs_one_request_per_call_same_precision"] = (
+            sat["requests_per_s"] / res["one_request_per_call_same_precision"]["requests_per_s"])
     for c in dcats + models + [dbase]:
         c.release()
     return res
@@ -603,6 +639,12 @@ def main():
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     t_all0 = torch.cuda.Event(enable_timing=True)
     t_all1 = torch.cuda.Event(enable_timing=True)
+    # the library records CUDA events around its passes on the launching stream (pass 1:
+    # the FP32C kernel, pass 2: the FP64 recomputation near critical curves)
+    timing = args.precision == "fp32c"
+    if timing:
+        ctx.set_pass_timing(True)
+        ctx.pass_times()
     barrier()
     n0 = lt.launch_count()
     with ClockSampler(gpu_id) as clocks:
@@ -617,6 +659,11 @@ def main():
     launches = lt.launch_count() - n0
     elapsed = t_all0.elapsed_time(t_all1) / 1e3
     per_launch = float(np.mean([s.elapsed_time(e) for s, e in zip(starts, ends)])) / 1e3
+    passes = None
+    if timing:
+        p1, p2, ncalls = ctx.pass_times()
+        ctx.set_pass_timing(False)
+        passes = {"pass1_ms": p1 / max(ncalls, 1), "pass2_ms": p2 / max(ncalls, 1), "calls": ncalls}
     evals_step = sums_per_pair * g.npix * cat.n
     value, elapsed, _ = replicas.throughput(evals_step * args.steps, elapsed, "cuda")
 
@@ -636,9 +683,15 @@ def main():
             dt = e0.elapsed_time(e1) / 1e3 / args.steps
             breakdown[label] = {"ms": dt * 1e3, "evals_per_s": g.npix * cat.n / dt}
 
-    # the same workload in LT_FP64 (the reference's FP64 arithmetic; Hessian bit-identical)
+    # the same workload in LT_FP64 (the reference's FP64 arithmetic; Hessian bit-identical),
+    # and the accuracy of the timed step's maps against it (max and RMS error per map,
+    # pixels with |mu| > 100 apart)
     fp64_cmp = None
+    errors = None
     if rank == 0 and args.precision != "fp64" and not args.no_fp64_compare:
+        from lenstool_hpc_b200.accuracy import map_errors
+        timed_maps = {k: v.clone() for k, v in outs.items()}  # the last timed step's output
+
         def time_precision(prec, k=2):
             maps_call(dcat, prec, outs, stream)
             f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -649,11 +702,19 @@ def main():
             ctx.synchronize(stream)
             return f0.elapsed_time(f1) / 1e3 / k
         t64 = time_precision("fp64")
+        errors = {"reference": "LT_FP64 on the same catalogue and grid (Hessian = the reference's CPU arithmetic "
+                               "bit for bit, potential = the reference's pi05)",
+                  "metric": "|got - fp64| / max(|fp64|, RMS of the map over |mu| <= 100)",
+                  args.precision: map_errors(timed_maps, outs)}
         fp64_cmp = {"evals_per_s": evals_step / t64, "ms_per_step": t64 * 1e3, "steps": 2,
                     "speedup_of_" + args.precision: (evals_step * args.steps / elapsed) / (evals_step / t64)}
         if args.precision != "fp64fast":
+            fp64_maps = {k: v.clone() for k, v in outs.items()}
             tf = time_precision("fp64fast")
             fp64_cmp["fp64fast"] = {"evals_per_s": evals_step / tf, "ms_per_step": tf * 1e3, "steps": 2}
+            errors["fp64fast"] = map_errors(outs, fp64_maps)
+            del fp64_maps
+        del timed_maps
 
     # end to end through the public API with host buffers: catalogue upload from host
     # arrays and the maps copied back into pinned host memory, every step
@@ -687,14 +748,22 @@ def main():
         fpp = {"all": FLOPS_PER_PAIR, "hessian": 182, "potential": 760}.get(args.maps)  # no census: deflection
         achieved = g.npix * cat.n * fpp / per_launch / 1e12 if fpp else None
         out_bytes = len(names) * g.npix * 8
+        cat_bytes = (256 + 160) * cat.n  # FP64 records (256 B) + FP32C records (160 B) per halo, at most
         pairs = g.npix * cat.n
         issue = args.precision == "fp32c" and args.maps == "all"
         if issue:
-            # the FMA-chain kernel issues one warp instruction per SMSP per cycle, the issue
-            # port's own rate: its flops / 2 is the peak of thread instructions per second
-            peak_inst = peak_tflops / 2 if peak_tflops else None
-            achieved_inst = pairs * INST_PER_PAIR_FP32C_LENS / per_launch / 1e12
-            fp32_tflops = pairs * FP32_FLOPS_PER_PAIR_FP32C_LENS / per_launch / 1e12
+            # pass 1 (the dominant kernel, grid32c_kernel<OP_HESS|OP_POT>) timed live by the
+            # library's events; its issued thread instructions per pair from ncu on the build
+            # whose sources KERNEL_SOURCES hash to INST_SOURCES_SHA.  Peak: every SMSP issues
+            # one warp instruction (32 thread instructions) per cycle, at the SM clock sampled
+            # during the timed region
+            t1 = passes["pass1_ms"] / 1e3 if passes and passes["calls"] else per_launch
+            sm_mhz = clocks.summary().get("sm_mhz") or 1965.0
+            nsm = torch.cuda.get_device_properties(local_rank).multi_processor_count
+            peak_inst = nsm * 4 * 32 * sm_mhz * 1e6 / 1e12
+            achieved_inst = pairs * INST_PER_PAIR_FP32C_LENS / t1 / 1e12
+            fp32_tflops = pairs * FP32_FLOPS_PER_PAIR_FP32C_LENS / t1 / 1e12
+            sources_now = kernel_sources_sha()
         cpu = None
         if not args.no_cpu_baseline:
             try:
@@ -711,18 +780,23 @@ def main():
                        "grid": f"{g.nx}x{g.ny} over 300\"x300\"", "halos": cat.n,
                        "maps": list(names), "precision": args.precision, "evals_per_step": evals_step,
                        "parallelism": f"replicas x{world}",
-                       "l2": "outputs 671 MB per step > 126 MB L2; catalogue 192 KB stays resident"},
+                       "l2": f"outputs {out_bytes / 1e6:.0f} MB per step > 126 MB L2 (no flush needed); catalogue "
+                             f"{cat_bytes / 1e3:.0f} KB stays resident"},
             "gpu_launches": int(launches),
             "roofline": ({"bound": "issue", "achieved": achieved_inst, "peak": peak_inst,
                           "unit": "T thread-instructions/s",
                           "frac": achieved_inst / peak_inst if peak_inst else None,
                           "inst_per_pair": INST_PER_PAIR_FP32C_LENS,
+                          "inst_per_pair_sources_sha": INST_SOURCES_SHA, "kernel_sources_sha": sources_now,
+                          "inst_per_pair_current": INST_SOURCES_SHA == sources_now,
                           "fp32": {"flops_per_pair": FP32_FLOPS_PER_PAIR_FP32C_LENS, "achieved": fp32_tflops,
                                    "peak": peak_tflops, "unit": "TFLOP/s",
-                                   "frac": fp32_tflops / peak_tflops if peak_tflops else None},
-                          "peak_source": "measured in-run: fp32 FMA-chain kernel (one warp instruction per "
-                                         "SMSP per cycle)",
-                          "time_basis": "whole step (pass 1 is ~95% of it)"} if issue else
+                                   "frac": fp32_tflops / peak_tflops if peak_tflops else None,
+                                   "peak_source": "measured in-run: fp32 FMA-chain kernel"},
+                          "peak_source": f"nominal issue rate: {nsm} SMs x 4 SMSPs x 32 lanes x the sampled "
+                                         f"SM clock ({sm_mhz:.0f} MHz)",
+                          "time_basis": "pass 1 alone, CUDA events on the launching stream over the timed "
+                                        "region", "passes": passes} if issue else
                          {"bound": pipe, "achieved": achieved, "peak": peak_tflops, "unit": "TFLOP/s",
                           "frac": achieved / peak_tflops if (peak_tflops and achieved) else None,
                           "flops_per_pair": fpp, "flop_convention": "weighted census of the reference's formulas",
@@ -744,6 +818,8 @@ def main():
             line["cpu_baseline"] = cpu
         if fp64_cmp:
             line["fp64_same_workload"] = fp64_cmp
+        if errors:
+            line["errors"] = errors
         if world == 1 and not args.skip_batch:
             line["posterior_batch"] = bench_posterior_batch(ctx, args.precision, steps=2, warmup=3,
                                                             n_sets=args.batch_sets)
@@ -755,6 +831,15 @@ def main():
     ctx.close()
     replicas.finalize()
     return 0
+
+
+def kernel_sources_sha() -> str:
+    """sha256 (16 hex digits) of the sources the FP32C lens-maps kernel is built from."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update((ROOT / "lenstool-hpc_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()[:16]
 
 
 def fma_peak_tflops(pipe: str) -> float:

@@ -261,10 +261,33 @@ lt_status lt_set_kernel_shape(lt_context *ctx, int32_t precision, int32_t sums, 
                               int32_t ctas_per_sm);
 lt_status lt_get_kernel_shape(const lt_context *ctx, int32_t precision, int32_t sums, int32_t *pixels_per_thread,
                               int32_t *ctas_per_sm);
-/* Time every shape for (precision, sums) on a grid_n x grid_n grid covering the
- * catalogue and keep the fastest in the context; *best_ms (may be NULL) gets its time. */
+/* The full kernel configuration: besides the shape, the threads per CTA (128 or 256; a
+ * tile is 32 x pixels_per_thread columns by threads / 32 rows) and the halo records per
+ * shared-memory stage (32, 64 or 128).  LT_FP32C kernels come in the shapes
+ * (pixels, CTAs/SM, threads) = (1|2, 1|2, 256), (1, 2|4, 128), (2, 2|3|4, 128), each with
+ * every stage size; the FP64 kernels in their four 256-thread, 64-record shapes.  An
+ * unbuilt configuration is LT_ERR_INVALID_ARGUMENT.  lt_set_kernel_shape keeps 256 threads
+ * and 64-record stages. */
+typedef struct {
+    int32_t pixels_per_thread, ctas_per_sm, threads, chunk;
+} lt_kernel_config;
+lt_status lt_set_kernel_config(lt_context *ctx, int32_t precision, int32_t sums, const lt_kernel_config *config);
+lt_status lt_get_kernel_config(const lt_context *ctx, int32_t precision, int32_t sums, lt_kernel_config *config);
+/* Time every configuration for (precision, sums) on a grid_n x grid_n grid covering the
+ * catalogue and keep the fastest in the context; *best_ms (may be NULL) gets its time.
+ * The batches built afterwards use the tuned LT_FP32C Hessian shape where their
+ * persistent kernel is built for it (pixels per thread and CTAs per SM at 256 threads). */
 lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision, int32_t sums, int32_t grid_n,
                       double *best_ms);
+
+/* ---- pass timing --------------------------------------------------------------------
+ * With timing on, every LT_FP32C grid call records CUDA events on its stream around its
+ * two passes (pass 1: the FP32C kernel; pass 2: the FP64 recomputation of the pixels
+ * near critical curves).  lt_pass_times waits for the last recorded call, returns the
+ * summed durations (ms) and the number of calls since the previous read, and starts a
+ * new count.  No counterpart in the reference. */
+lt_status lt_set_pass_timing(lt_context *ctx, int32_t on);
+lt_status lt_pass_times(lt_context *ctx, double *pass1_ms, double *pass2_ms, int32_t *calls);
 
 /* ---- requests: batches and the serving loop ----------------------------------------
  * A request is one grid of output planes over one uploaded catalogue: any mix of Hessian
@@ -291,6 +314,10 @@ lt_status lt_batch_create(lt_context *ctx, const lt_request *reqs, int32_t nreqs
 /* Replay the batch's graph on `stream` (asynchronous; lt_synchronize reports errors). */
 lt_status lt_batch_launch(lt_context *ctx, lt_batch *batch, void *stream);
 int32_t lt_batch_size(const lt_batch *batch);
+/* The batch's kernel configuration: its persistent kernel's pixels per thread and CTAs
+ * per SM for LT_FP32C tiles (taken at lt_batch_create from the context's LT_FP32C Hessian
+ * shape, as lt_autotune left it), 256 threads, 64-record stages. */
+lt_status lt_batch_config(const lt_batch *batch, lt_kernel_config *config);
 lt_status lt_batch_destroy(lt_context *ctx, lt_batch *batch);
 
 typedef struct lt_server lt_server;
@@ -302,6 +329,9 @@ typedef struct {
     int32_t idle_us;      /* idle time after which the persistent kernel leaves (0: 20000) */
     size_t output_bytes;  /* HBM arena staging host-pointer outputs: the admission budget  */
                           /* (0: 4 GiB)                                                    */
+    int32_t descriptor_wait_us; /* the loop's bounded wait for the descriptor of a published
+                                   request (~1 us polls, 0: 2 s); when it runs out the request
+                                   fails with LT_ERR_TIMEOUT and the loop serves the rest   */
 } lt_server_config;
 
 typedef struct {
@@ -309,6 +339,7 @@ typedef struct {
     int32_t max_inflight, inflight, queued, loop_running;
     size_t arena_bytes, arena_peak;
     uint64_t device_published, device_head; /* the queue's counters as the device sees them */
+    uint64_t timed_out;   /* requests failed because their descriptor never reached the device */
 } lt_server_stats;
 
 /* Start a serving loop on the context.  While it runs, lt_catalog_release defers the
@@ -334,6 +365,13 @@ lt_status lt_server_release(lt_server *server, uint64_t ticket);
 lt_status lt_server_get_stats(lt_server *server, lt_server_stats *stats);
 /* Finish every submitted request, stop the loop and free the server. */
 lt_status lt_server_destroy(lt_server *server);
+/* Failure injection on the host, for tests of the loop's bounded waits:
+ * LT_FAULT_DROP_DESCRIPTOR publishes the next admitted request without copying its
+ * descriptor to the device (a lost message), so the loop's wait for it runs out and the
+ * request fails with LT_ERR_TIMEOUT while later requests are served.  No counterpart in
+ * the reference (its GPU calls exit on error, src/grid_gradient_GPU.cu:48-51). */
+#define LT_FAULT_DROP_DESCRIPTOR 1
+lt_status lt_server_inject_fault(lt_server *server, int32_t fault);
 
 /* ---- Hessian maps without allocation ------------------------------------------------
  * lt_hessian_maps in LT_FP32C with device outputs, for callers that must not allocate
@@ -346,8 +384,10 @@ lt_status lt_server_destroy(lt_server *server);
  * per process and device, so calls that overlap in time race on it and must be
  * serialised by the caller.  The first call on a device looks up the array's address
  * (cudaGetSymbolAddress, return code checked) and loads the module's data there; make
- * that first call before any stream capture that includes this call.  No counterpart in
- * the reference. */
+ * that first call before any stream capture that includes this call.  The address is
+ * kept until the last context of the device is destroyed (lt_destroy); a device reset
+ * (cudaDeviceReset) while a context lives invalidates it, so the call must not be used
+ * across a reset.  No counterpart in the reference. */
 lt_status lt_hessian_maps_noalloc(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid, int32_t kmap,
                                   double dlsds, double mult, const lt_map_request *maps, int32_t nmaps,
                                   void *stream);

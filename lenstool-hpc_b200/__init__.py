@@ -77,7 +77,7 @@ class _Request(C.Structure):
 
 class _ServerConfig(C.Structure):
     _fields_ = [("precision", C.c_int32), ("slots", C.c_int32), ("window", C.c_int32), ("idle_us", C.c_int32),
-                ("output_bytes", C.c_size_t)]
+                ("output_bytes", C.c_size_t), ("descriptor_wait_us", C.c_int32)]
 
 
 class _ServerStats(C.Structure):
@@ -85,7 +85,7 @@ class _ServerStats(C.Structure):
                 ("failed", C.c_uint64), ("loop_launches", C.c_uint64), ("max_inflight", C.c_int32),
                 ("inflight", C.c_int32), ("queued", C.c_int32), ("loop_running", C.c_int32),
                 ("arena_bytes", C.c_size_t), ("arena_peak", C.c_size_t), ("device_published", C.c_uint64),
-                ("device_head", C.c_uint64)]
+                ("device_head", C.c_uint64), ("timed_out", C.c_uint64)]
 
 
 class _HaloParams(C.Structure):
@@ -116,6 +116,11 @@ class _Systems(C.Structure):
 MAX_IMAGES = 20
 
 
+class _KernelConfig(C.Structure):
+    _fields_ = [("pixels_per_thread", C.c_int32), ("ctas_per_sm", C.c_int32), ("threads", C.c_int32),
+                ("chunk", C.c_int32)]
+
+
 class _Cosmo(C.Structure):
     _fields_ = [("model", C.c_int32), ("omegaM", C.c_double), ("omegaX", C.c_double), ("curvature", C.c_double),
                 ("wX", C.c_double), ("wa", C.c_double), ("H0", C.c_double)]
@@ -127,13 +132,15 @@ _LIB = None
 EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release", "lt_catalog_nhalos",
            "lt_gradient_grid", "lt_hessian_maps", "lt_potential_grid", "lt_lens_maps", "lt_synchronize",
            "lt_cosmo_distances", "lt_kernel_launch_count", "lt_status_string", "lt_last_error", "lt_abi_version",
-           "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_autotune", "lt_measure_fma_peak",
-           "lt_batch_create", "lt_batch_launch", "lt_batch_size", "lt_batch_destroy", "lt_server_create",
+           "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_set_kernel_config", "lt_get_kernel_config",
+           "lt_autotune", "lt_measure_fma_peak", "lt_set_pass_timing", "lt_pass_times",
+           "lt_batch_create", "lt_batch_launch", "lt_batch_size", "lt_batch_config", "lt_batch_destroy",
+           "lt_server_create",
            "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
            "lt_server_get_stats", "lt_server_destroy", "lt_chi2", "lt_chi2_batch", "lt_delense",
            "lt_catalog_update", "lt_write_fits", "lt_eval_fast_math", "lt_eval_fast_math32", "lt_bayes_create",
            "lt_bayes_apply", "lt_bayes_destroy", "lt_chi2_batch_precision", "lt_server_submit_chi2",
-           "lt_server_chi2_result")
+           "lt_server_chi2_result", "lt_server_inject_fault")
 SUMS = {"deflection": 1, "hessian": 2, "potential": 4, "lens": 6}
 
 
@@ -161,12 +168,17 @@ def load_library(path=None):
     L.lt_cosmo_distances.argtypes = [C.POINTER(_Cosmo), C.c_double, C.c_double, _dp, _dp, _dp]
     L.lt_set_kernel_shape.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
     L.lt_get_kernel_shape.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+    L.lt_set_kernel_config.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(_KernelConfig)]
+    L.lt_get_kernel_config.argtypes = [vp, C.c_int32, C.c_int32, C.POINTER(_KernelConfig)]
     L.lt_autotune.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+    L.lt_set_pass_timing.argtypes = [vp, C.c_int32]
+    L.lt_pass_times.argtypes = [vp, _dp, _dp, _ip]
     L.lt_measure_fma_peak.argtypes = [C.c_int, C.c_int]
     L.lt_measure_fma_peak.restype = C.c_double
     L.lt_batch_create.argtypes = [vp, C.POINTER(_Request), C.c_int32, C.c_int32, C.POINTER(vp)]
     L.lt_batch_launch.argtypes = [vp, vp, vp]
     L.lt_batch_size.argtypes = [vp]
+    L.lt_batch_config.argtypes = [vp, C.POINTER(_KernelConfig)]
     L.lt_batch_destroy.argtypes = [vp, vp]
     L.lt_server_create.argtypes = [vp, C.POINTER(_ServerConfig), C.POINTER(vp)]
     L.lt_server_submit.argtypes = [vp, C.POINTER(_Request), C.POINTER(C.c_uint64)]
@@ -176,6 +188,7 @@ def load_library(path=None):
     L.lt_server_release.argtypes = [vp, C.c_uint64]
     L.lt_server_get_stats.argtypes = [vp, C.POINTER(_ServerStats)]
     L.lt_server_destroy.argtypes = [vp]
+    L.lt_server_inject_fault.argtypes = [vp, C.c_int32]
     L.lt_server_submit_chi2.argtypes = [vp, vp, C.POINTER(_Frame), C.c_int32, C.POINTER(_Systems),
                                         C.POINTER(C.c_uint64)]
     L.lt_server_chi2_result.argtypes = [vp, C.c_uint64, _dp, _ip]
@@ -391,15 +404,36 @@ class Context:
         self._check(st, "lt_get_kernel_shape")
         return a.value, b.value
 
+    def set_kernel_config(self, precision, sums, pixels_per_thread, ctas_per_sm, threads=256, chunk=64):
+        c = _KernelConfig(pixels_per_thread, ctas_per_sm, threads, chunk)
+        st = self._lib.lt_set_kernel_config(self.handle, PRECISION[precision], SUMS.get(sums, sums), C.byref(c))
+        self._check(st, "lt_set_kernel_config")
+
+    def kernel_config(self, precision, sums) -> dict:
+        c = _KernelConfig()
+        st = self._lib.lt_get_kernel_config(self.handle, PRECISION[precision], SUMS.get(sums, sums), C.byref(c))
+        self._check(st, "lt_get_kernel_config")
+        return {f: getattr(c, f) for f, _ in _KernelConfig._fields_}
+
     def autotune(self, cat, precision="fp32c", sums="lens", grid_n=512):
-        """Time every kernel shape on a grid_n^2 grid over the catalogue; keep the fastest.
-        Returns (pixels_per_thread, ctas_per_sm, ms)."""
+        """Time every kernel configuration on a grid_n^2 grid over the catalogue; keep the
+        fastest.  Returns (pixels_per_thread, ctas_per_sm, ms); kernel_config() gives the
+        threads per CTA and the stage size too."""
         cat = self._cat(cat)
         ms = C.c_double()
         st = self._lib.lt_autotune(self.handle, cat.handle, PRECISION[precision], SUMS.get(sums, sums), grid_n,
                                    C.byref(ms))
         self._check(st, "lt_autotune")
         return self.kernel_shape(precision, sums) + (ms.value,)
+
+    def set_pass_timing(self, on=True):
+        self._check(self._lib.lt_set_pass_timing(self.handle, int(bool(on))), "lt_set_pass_timing")
+
+    def pass_times(self):
+        """(pass-1 ms, pass-2 ms, calls) summed over the FP32C calls since the last read."""
+        a, b, n = C.c_double(), C.c_double(), C.c_int32()
+        self._check(self._lib.lt_pass_times(self.handle, C.byref(a), C.byref(b), C.byref(n)), "lt_pass_times")
+        return a.value, b.value, n.value
 
     def synchronize(self, stream=None):
         self._check(self._lib.lt_synchronize(self.handle, _stream_handle(stream)), "lt_synchronize")
@@ -447,9 +481,10 @@ class Context:
         self._check(st, "lt_batch_create")
         return Batch(self, h, reqs)
 
-    def server(self, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0) -> "Server":
+    def server(self, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0,
+               descriptor_wait_us=0) -> "Server":
         """lt_server_create: a continuous-batching serving loop on this context."""
-        return Server(self, precision, slots, window, idle_us, output_bytes)
+        return Server(self, precision, slots, window, idle_us, output_bytes, descriptor_wait_us)
 
     def bayes(self, model, columns, potfiles=()) -> "Bayes":
         """lt_bayes_create: a bayes.dat model (bayes.BayesModel), its potfiles
@@ -542,6 +577,12 @@ class Batch:
     def __len__(self):
         return int(self.ctx._lib.lt_batch_size(self.handle))
 
+    def config(self) -> dict:
+        """lt_batch_config: the persistent kernel's shape for this batch."""
+        c = _KernelConfig()
+        self.ctx._check(self.ctx._lib.lt_batch_config(self.handle, C.byref(c)), "lt_batch_config")
+        return {f: getattr(c, f) for f, _ in _KernelConfig._fields_}
+
     def launch(self, stream=None):
         self.ctx._check(self.ctx._lib.lt_batch_launch(self.ctx.handle, self.handle, _stream_handle(stream)),
                         "lt_batch_launch")
@@ -561,9 +602,10 @@ class Batch:
 class Server:
     """lt_server: continuous batching of map requests on one context."""
 
-    def __init__(self, ctx: Context, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0):
+    def __init__(self, ctx: Context, precision="fp32c", slots=0, window=0, idle_us=0, output_bytes=0,
+                 descriptor_wait_us=0):
         self.ctx, self._lib = ctx, ctx._lib
-        cfg = _ServerConfig(PRECISION[precision], slots, window, idle_us, output_bytes)
+        cfg = _ServerConfig(PRECISION[precision], slots, window, idle_us, output_bytes, descriptor_wait_us)
         h = C.c_void_p()
         st = self._lib.lt_server_create(ctx.handle, C.byref(cfg), C.byref(h))
         ctx._check(st, "lt_server_create")
@@ -620,6 +662,10 @@ class Server:
     def release(self, ticket: int):
         self._lib.lt_server_release(self.handle, ticket)
         self._keep.pop(ticket, None)
+
+    def inject_fault(self, fault: int = 1):
+        """lt_server_inject_fault (1: the next admitted request loses its descriptor)."""
+        self.ctx._check(self._lib.lt_server_inject_fault(self.handle, fault), "lt_server_inject_fault")
 
     def stats(self) -> dict:
         s = _ServerStats()

@@ -23,6 +23,7 @@ using namespace lt;
 
 struct lt_batch {
     int mode = 0;
+    int variant = 0; /* queue kernel variant (FP32C: pixels per thread, CTAs per SM) */
     int n = 0;
     QSlot *slots = nullptr;
     QState *state = nullptr;
@@ -48,8 +49,10 @@ static int public_kind(int k, int &op)
 
 /* Validate a request and fill its queue descriptor.  `outs` (may be NULL) replaces the
  * request's output pointers (the serving loop's staging planes for host outputs);
- * otherwise the request's outputs must be device pointers. */
-lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, double *const *outs, QItem *it)
+ * otherwise the request's outputs must be device pointers.  FP32C tiles have `ppt32`
+ * pixels per thread (the queue kernel variant's). */
+lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, double *const *outs, QItem *it,
+                          int ppt32)
 {
     if (!r || !r->cat || !grid_ok(&r->grid) || r->nmaps < 1 || r->nmaps > LT_MAX_MAPS) {
         set_error(ctx, "invalid request (catalogue, grid or map count)");
@@ -104,7 +107,7 @@ lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, d
     a.scale = r->scale;
     a.status = ctx->status;
     it->op = op;
-    it->ppt = c32 ? 2 : ((op & OP_POT) ? 1 : 2);
+    it->ppt = c32 ? (ppt32 == 1 ? 1 : 2) : ((op & OP_POT) ? 1 : 2);
     const int P = it->ppt;
     a.tiles_x = (a.nx + 32 * P - 1) / (32 * P);
     a.ntiles = a.tiles_x * ((a.ny + 7) / 8);
@@ -114,7 +117,7 @@ lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, d
         it->recs32 = fc.recs32;
         it->chunks32 = fc.chunks;
         it->nchunks32 = cat->nhalos ? fc.nchunks : 0;
-        it->mu_flag = det ? LT_FP32C_MU_FLAG : 0.0;
+        it->mu_tol = det ? kMuTol32 : 0.0;
     }
     if (cat->nhalos == 0) a.nchunks = 0;
     return LT_OK;
@@ -131,12 +134,14 @@ lt_status lt_batch_create(lt_context *ctx, const lt_request *reqs, int32_t nreqs
     *out = nullptr;
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
+    /* the queue kernel variant nearest to the context's (tuned) FP32C Hessian shape */
+    const int variant = queue_variant(ctx->shape[LT_FP32C][OP_HESS]);
     std::vector<QSlot> host((size_t)nreqs);
     std::vector<double> cost((size_t)nreqs);
     for (int i = 0; i < nreqs; i++) {
         QSlot &s = host[i];
         memset(&s, 0, sizeof(s));
-        lt_status st = make_queue_item(ctx, &reqs[i], precision, nullptr, &s.item);
+        lt_status st = make_queue_item(ctx, &reqs[i], precision, nullptr, &s.item, shape_ppt(variant));
         if (st != LT_OK) {
             set_error(ctx, "request %d: %s", i, lt_last_error(ctx));
             return st;
@@ -156,6 +161,7 @@ lt_status lt_batch_create(lt_context *ctx, const lt_request *reqs, int32_t nreqs
     lt_batch *b = new (std::nothrow) lt_batch();
     if (!b) return LT_ERR_OUT_OF_MEMORY;
     b->mode = precision == LT_FP32C ? QMODE_C32 : QMODE_EXACT;
+    b->variant = variant;
     b->n = nreqs;
     b->bytes = sizeof(QSlot) * (size_t)nreqs + sizeof(QState);
     void *mem = nullptr;
@@ -167,7 +173,7 @@ lt_status lt_batch_create(lt_context *ctx, const lt_request *reqs, int32_t nreqs
     b->state = (QState *)mem;
     b->slots = (QSlot *)((char *)mem + sizeof(QState));
     cudaError_t e = cudaMemcpy(b->slots, slots.data(), sizeof(QSlot) * (size_t)nreqs, cudaMemcpyHostToDevice);
-    const int blocks = queue_blocks(b->mode, ctx->num_sms);
+    const int blocks = queue_blocks(b->mode, b->variant, ctx->num_sms);
     cudaStream_t cs = nullptr;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
@@ -178,9 +184,10 @@ lt_status lt_batch_create(lt_context *ctx, const lt_request *reqs, int32_t nreqs
         q.nslots = nreqs;
         q.window = 1;
         q.idle_polls = 0;
+        q.desc_polls = 1 << 30; /* every descriptor is in place before the graph runs */
         q.status = ctx->status;
         launch_queue_reset(b->slots, b->state, nreqs, cs);
-        launch_queue(b->mode, q, blocks, cs);
+        launch_queue(b->mode, b->variant, q, blocks, cs);
         e = cudaStreamEndCapture(cs, &b->graph);
     }
     if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
@@ -206,6 +213,16 @@ lt_status lt_batch_launch(lt_context *ctx, lt_batch *b, void *stream)
 }
 
 int32_t lt_batch_size(const lt_batch *b) { return b ? b->n : -1; }
+
+lt_status lt_batch_config(const lt_batch *b, lt_kernel_config *c)
+{
+    if (!b || !c) return LT_ERR_INVALID_ARGUMENT;
+    c->pixels_per_thread = b->mode == QMODE_C32 ? shape_ppt(b->variant) : 0;
+    c->ctas_per_sm = b->mode == QMODE_C32 ? shape_cps(b->variant) : 2;
+    c->threads = 256;
+    c->chunk = LT_CHUNK;
+    return LT_OK;
+}
 
 lt_status lt_batch_destroy(lt_context *ctx, lt_batch *b)
 {

@@ -23,9 +23,29 @@
 using namespace lt;
 
 static std::atomic<uint64_t> g_launches{0};
+static std::mutex g_ctx_mu;
+static int g_contexts[64] = {}; /* live contexts per device (devices 0..63) */
 
 namespace lt {
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void pass_mark(lt_context *ctx, cudaStream_t stream, int which)
+{
+    (void)which;
+    if (!ctx->timing) return;
+    cudaEvent_t e;
+    if (ctx->ev_pool.empty()) {
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            return;
+        }
+    } else {
+        e = ctx->ev_pool.back();
+        ctx->ev_pool.pop_back();
+    }
+    cudaEventRecord(e, stream);
+    ctx->ev_marks.push_back(e);
+}
 } // namespace lt
 
 /* ------------------------------------------------------------------ helpers ---- */
@@ -233,8 +253,9 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
     if (!ctx) return LT_ERR_OUT_OF_MEMORY;
     ctx->device = device;
     ctx->num_sms = prop.multiProcessorCount;
-    /* default kernel shapes (pixels per thread, CTAs per SM), from a sweep on B200 at
-     * 1024^2 x 1000 halos; lt_autotune refines them for a given catalogue */
+    /* default kernel shapes (pixels per thread, CTAs per SM, threads, records per stage),
+     * from sweeps on B200 of the 1000-halo workload; lt_autotune refines them for a given
+     * catalogue */
     for (int p = 0; p < 3; p++)
         for (int o = 0; o < 8; o++) ctx->shape[p][o] = LT_SHAPE(2, 1);
     ctx->shape[LT_FP64][OP_HESS] = LT_SHAPE(2, 2);
@@ -245,10 +266,10 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
     ctx->shape[LT_FP64_FAST][OP_POT] = LT_SHAPE(1, 2);
     ctx->shape[LT_FP64_FAST][OP_HESS | OP_POT] = LT_SHAPE(1, 2);
     ctx->shape[LT_FP64_FAST][OP_GRAD] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP32C][OP_HESS] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP32C][OP_HESS | OP_POT] = LT_SHAPE(2, 2);
-    ctx->shape[LT_FP32C][OP_GRAD] = LT_SHAPE(2, 2);
+    ctx->shape[LT_FP32C][OP_HESS] = LT_SHAPE4(2, 2, 256, 128);
+    ctx->shape[LT_FP32C][OP_POT] = LT_SHAPE4(2, 2, 256, 128);
+    ctx->shape[LT_FP32C][OP_HESS | OP_POT] = LT_SHAPE4(2, 2, 256, 128);
+    ctx->shape[LT_FP32C][OP_GRAD] = LT_SHAPE4(2, 2, 256, 128);
     cudaSetDevice(device);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
@@ -260,6 +281,10 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
         return st;
     }
     cudaMemset(ctx->status, 0, 64);
+    if (device < 64) {
+        std::lock_guard<std::mutex> lock(g_ctx_mu);
+        g_contexts[device]++;
+    }
     *out = ctx;
     return LT_OK;
 }
@@ -273,8 +298,53 @@ lt_status lt_destroy(lt_context *ctx)
     dev_free(ctx, ctx->list, ctx->list_bytes);
     dev_free(ctx, ctx->status, 64);
     destroy_extensions(ctx);
+    for (cudaEvent_t e : ctx->ev_marks) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
+    if (ctx->device < 64) {
+        std::lock_guard<std::mutex> lock(g_ctx_mu);
+        if (--g_contexts[ctx->device] == 0) noalloc_forget(ctx->device);
+    }
     delete ctx;
     return LT_OK;
+}
+
+lt_status lt_set_pass_timing(lt_context *ctx, int32_t on)
+{
+    if (!ctx) return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    ctx->timing = on != 0;
+    if (!ctx->timing) {
+        for (cudaEvent_t e : ctx->ev_marks) ctx->ev_pool.push_back(e);
+        ctx->ev_marks.clear();
+    }
+    return LT_OK;
+}
+
+lt_status lt_pass_times(lt_context *ctx, double *pass1_ms, double *pass2_ms, int32_t *calls)
+{
+    if (!ctx || !pass1_ms || !pass2_ms || !calls) return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    *pass1_ms = *pass2_ms = 0.;
+    *calls = 0;
+    const size_t n = ctx->ev_marks.size() / 3 * 3;
+    lt_status st = LT_OK;
+    if (n) {
+        cudaError_t e = cudaEventSynchronize(ctx->ev_marks[n - 1]);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, "pass timing");
+    }
+    for (size_t i = 0; st == LT_OK && i < n; i += 3) {
+        float a = 0.f, b = 0.f;
+        cudaEventElapsedTime(&a, ctx->ev_marks[i], ctx->ev_marks[i + 1]);
+        cudaEventElapsedTime(&b, ctx->ev_marks[i + 1], ctx->ev_marks[i + 2]);
+        *pass1_ms += a;
+        *pass2_ms += b;
+        ++*calls;
+    }
+    for (cudaEvent_t e : ctx->ev_marks) ctx->ev_pool.push_back(e);
+    ctx->ev_marks.clear();
+    return st;
 }
 
 lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *s, lt_catalog **out)
@@ -558,8 +628,39 @@ lt_status lt_get_kernel_shape(const lt_context *ctx, int32_t precision, int32_t 
 {
     if (!ctx || !ppt || !cps || !sums_ok(precision, sums)) return LT_ERR_INVALID_ARGUMENT;
     const int s = ctx->shape[precision][sums];
-    *ppt = s & 15;
-    *cps = s >> 4;
+    *ppt = shape_ppt(s);
+    *cps = shape_cps(s);
+    return LT_OK;
+}
+
+static bool config_ok(int precision, const lt_kernel_config *c)
+{
+    if (!c) return false;
+    const int s = LT_SHAPE4(c->pixels_per_thread, c->ctas_per_sm, c->threads, c->chunk);
+    if (c->pixels_per_thread < 1 || c->pixels_per_thread > 2 || c->ctas_per_sm < 1 || c->ctas_per_sm > 4 ||
+        (c->threads != 128 && c->threads != 256) || (c->chunk != 32 && c->chunk != 64 && c->chunk != 128))
+        return false;
+    if (precision == LT_FP32C) return shape32_ok(s);
+    /* the FP64 kernels come in the four (pixels, CTAs) shapes at 256 threads, 64-record stages */
+    return c->threads == 256 && c->chunk == 64 && c->ctas_per_sm <= 2;
+}
+
+lt_status lt_set_kernel_config(lt_context *ctx, int32_t precision, int32_t sums, const lt_kernel_config *c)
+{
+    if (!ctx || !sums_ok(precision, sums) || !config_ok(precision, c)) return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->shape[precision][sums] = LT_SHAPE4(c->pixels_per_thread, c->ctas_per_sm, c->threads, c->chunk);
+    return LT_OK;
+}
+
+lt_status lt_get_kernel_config(const lt_context *ctx, int32_t precision, int32_t sums, lt_kernel_config *c)
+{
+    if (!ctx || !c || !sums_ok(precision, sums)) return LT_ERR_INVALID_ARGUMENT;
+    const int s = ctx->shape[precision][sums];
+    c->pixels_per_thread = shape_ppt(s);
+    c->ctas_per_sm = shape_cps(s);
+    c->threads = shape_threads(s);
+    c->chunk = shape_cap(s);
     return LT_OK;
 }
 
@@ -596,14 +697,22 @@ lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision,
         if (st != LT_OK) return st;
     }
     double *outs[2] = {planes, planes + (size_t)grid_n * grid_n};
-    const int shapes[4] = {LT_SHAPE(1, 1), LT_SHAPE(1, 2), LT_SHAPE(2, 1), LT_SHAPE(2, 2)};
+    /* the search space: FP32C every built shape (pixels per thread, CTAs per SM, threads
+     * per CTA) with every stage size; the FP64 kernels their four (pixels, CTAs) shapes */
+    std::vector<int> shapes;
+    if (precision == LT_FP32C) {
+        for (int k = 0; k < kNumShapes32; k++)
+            for (int cap : {32, 64, 128}) shapes.push_back((kShapes32[k] & 0xffff) | ((cap / 32) << 16));
+    } else {
+        shapes = {LT_SHAPE(1, 1), LT_SHAPE(1, 2), LT_SHAPE(2, 1), LT_SHAPE(2, 2)};
+    }
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     double best = 1e300;
     int best_shape = ctx->shape[precision][sums];
     lt_status st = LT_OK;
-    for (int k = 0; k < 4 && st == LT_OK; k++) {
+    for (size_t k = 0; k < shapes.size() && st == LT_OK; k++) {
         ctx->shape[precision][sums] = shapes[k];
         st = run_grid(ctx, cat, &g, precision, sums, 0, 1.0, 1.0, 1.0, nout, kinds, outs, nullptr);
         if (st != LT_OK) break;

@@ -46,9 +46,16 @@ struct GridArgs {
     int32_t list_cap;
 };
 
-/* Kernel shape: pixels per thread (1 or 2) and resident CTAs per SM the register budget
- * is cut for (1 or 2). */
-#define LT_SHAPE(ppt, cps) ((ppt) | ((cps) << 4))
+/* Kernel shape: pixels per thread (1 or 2), resident CTAs per SM the register budget is
+ * cut for (1-4), threads per CTA (128 or 256) and halo records per shared-memory stage
+ * (32, 64 or 128).  LT_SHAPE keeps 256 threads and 64-record stages. */
+#define LT_SHAPE4(ppt, cps, nt, cap) ((ppt) | ((cps) << 4) | (((nt) / 32) << 8) | (((cap) / 32) << 16))
+#define LT_SHAPE(ppt, cps) LT_SHAPE4(ppt, cps, 256, 64)
+
+inline int shape_ppt(int s) { return s & 15; }
+inline int shape_cps(int s) { return (s >> 4) & 15; }
+inline int shape_threads(int s) { return ((s >> 8) & 255) * 32; }
+inline int shape_cap(int s) { return ((s >> 16) & 15) * 32; }
 
 /* Launch the FP64 grid kernel for the sums in `op` (OP_* mask).  Returns the CUDA error. */
 int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode = false,

@@ -24,7 +24,11 @@ struct lt_context {
     void *ext = nullptr;       /* state of the batch and serving extensions */
     void *list = nullptr;      /* pixel list of the FP32C recomputation pass (+ count) */
     size_t list_bytes = 0;
-    int shape[3][8] = {};      /* kernel shape per [precision][sums mask], LT_SHAPE() */
+    int shape[3][8] = {};      /* kernel shape per [precision][sums mask], LT_SHAPE4() */
+    /* pass timing (lt_set_pass_timing): CUDA events around the passes of FP32C calls */
+    bool timing = false;
+    std::vector<cudaEvent_t> ev_pool;   /* created events, reused */
+    std::vector<cudaEvent_t> ev_marks;  /* recorded marks: triples (start, pass 1 end, pass 2 end) */
 };
 
 struct lt_catalog {
@@ -45,24 +49,38 @@ struct lt_catalog {
 
 struct lt_rec32;
 
-/* FP32C: pixels with |mu| above this are recomputed in FP64 (the FP32C error of mu grows
- * as mu^2 near critical curves) */
-#define LT_FP32C_MU_FLAG 2.5
 
 namespace lt {
+
+/* FP32C: a pixel whose bound on the FP32 part's relative error of mu, |d det| / |det|,
+ * exceeds this is recomputed in FP64 (near a critical curve the determinant amplifies
+ * the error of the sums as |mu|) */
+constexpr double kMuTol32 = 4.0e-7;
 
 /* FP32C catalogue (lt_catalog::aux_desc): FP32 records + a chunk list over both record
  * kinds (chunk.pad & CHUNK_FP32: FP32 records of recs32, else FP64 records of recs64). */
 struct Fp32cCatalog {
     lt_rec32 *recs32;
-    lt_chunk *chunks;
-    int32_t nchunks;
+    lt_chunk *chunks;   /* chunks of at most 64 records */
+    lt_chunk *chunks_s; /* the same records in chunks of at most 32 */
+    lt_chunk *chunks_l; /* ... and of at most 128 */
+    int32_t nchunks, nchunks_s, nchunks_l;
     int32_t n32;
     int32_t *idx32;  /* per halo: its FP32 record, or -1 for an FP64-class halo (device) */
     int32_t *types;  /* per halo profile type (device) */
 };
 
 void count_launch(uint64_t n);
+/* With pass timing on, record mark `which` (0: before pass 1, 1: after it, 2: after
+ * pass 2) on `stream`; a call without pass 2 repeats mark 1 as mark 2. */
+void pass_mark(lt_context *ctx, cudaStream_t stream, int which);
+/* lt_hessian_maps_noalloc: forget the static list's address on `device` (its last
+ * context is being destroyed) */
+void noalloc_forget(int device);
+/* FP32C kernel shapes the library is built for */
+extern const int kShapes32[];
+extern const int kNumShapes32;
+bool shape32_ok(int shape);
 void set_error(lt_context *ctx, const char *fmt, ...);
 lt_status cuda_fail(lt_context *ctx, cudaError_t e, const char *what);
 lt_status dev_alloc(lt_context *ctx, void **p, size_t bytes);

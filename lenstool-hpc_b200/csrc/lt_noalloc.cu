@@ -14,7 +14,8 @@
  * The list's length word must start at zero; the call zeroes it on its stream before
  * pass 1.  The array's address is looked up once per device (cudaGetSymbolAddress with
  * that device current); that first call also loads the module's data on the device, so
- * it should come before any stream capture that includes this call.
+ * it should come before any stream capture that includes this call.  The address is
+ * forgotten when the last context of the device is destroyed.
  */
 #include <cstring>
 #include <mutex>
@@ -59,6 +60,17 @@ lt_status list_address(lt_context *ctx, int32_t **out)
     return LT_OK;
 }
 } // namespace
+
+namespace lt {
+/* Called by lt_destroy for the last context of a device: the next call looks the array
+ * up again (after a device reset its module, and so its address, is new). */
+void noalloc_forget(int device)
+{
+    if (device < 0 || device >= kMaxDevices) return;
+    std::lock_guard<std::mutex> lock(g_lookup_mu);
+    g_list_addr[device] = nullptr;
+}
+} // namespace lt
 
 extern "C" lt_status lt_hessian_maps_noalloc(lt_context *ctx, const lt_catalog *cat, const lt_grid *grid,
                                               int32_t kmap, double dlsds, double mult, const lt_map_request *maps,

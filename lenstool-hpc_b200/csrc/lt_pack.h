@@ -11,7 +11,7 @@
  * (src/gradient.cpp:764-783, src/gradient2.cpp:57-66, src/potential_GPU.cu:52-58) and the
  * potential parameters of module_readParameters_calculatePotentialparameter
  * (src/module_readParameters.cpp:2808-2871); the FP32 records carry the invariants of the
- * FP32 forms (lt_profiles32.cuh) and the FP64-fallback radii.
+ * FP32 closed forms (lt_profiles32.cuh) and the FP64-fallback radius.
  */
 #pragma once
 #include <math.h>
@@ -39,10 +39,8 @@ inline double sqr(double a) { return sqrt(a); }
 inline float f32(double a) { return (float)a; }
 #endif
 
-/* FP64 (halo-wide) thresholds of the FP32C path */
+/* FP64 regions of the FP32C path */
 constexpr double kTau = 0.1;       /* FP64 where b0 / (2 r) > kTau                        */
-constexpr double kSingFrac = 0.3;  /* FP64 within (kSingFrac + kSingEps e) r of the       */
-constexpr double kSingEps = 1.5;   /*   singular point of radius r                        */
 constexpr double kCoreFrac = 3.0;  /* FP64 within 3 rcore of the centre                   */
 
 /* b0 and ellipticity_potential from the velocity dispersion and the mass ellipticity
@@ -157,7 +155,10 @@ LT_HD inline bool needs_fp64_always(const lt_rec64 &r, int type)
     return false;
 }
 
-/* The FP32 record of an FP32-class halo (the invariants of lt_profiles32.cuh). */
+/* The FP32 record of an FP32-class halo (the invariants of the closed forms of
+ * lt_profiles32.cuh: q = (1-e)/(1+e), k = sqrt(1 - q^2) = 2 sqrt(e)/(1+e), s = (1+e) r,
+ * A = b0 (1-e) t05) and its FP64 disc: the larger of the near field (b0 / 2r > kTau) and
+ * kCoreFrac core radii. */
 LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
 {
     memset(&o, 0, sizeof(o));
@@ -174,45 +175,47 @@ LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     const double near_r = div(r.b0, mul(2., kTau));
     o.rnear2 = f32(mul(near_r, near_r));
     if (type == 5) {
-        o.cx1 = f32(sub(1., e));
-        o.icx1 = f32(add(1., e));
-        o.kpre = f32(mul(mul(r.b0, sub(1., e)), add(1., e)));
-        o.ppre = f32(r.b0);
+        o.q2 = f32(sub(1., e));
+        o.k = f32(add(1., e));
+        o.K = f32(mul(mul(r.b0, sub(1., e)), add(1., e)));
+        o.Ak = f32(r.b0);
         return;
     }
-    const double sqe = sqr(e);
-    const double cx1 = div(sub(1., e), add(1., e));
-    const double ci = div(mul(0.5, sub(1., mul(e, e))), sqe);
+    const double ope = add(1., e), ome = sub(1., e);
+    const double q = div(ome, ope), q2 = mul(q, q), opq2 = add(1., q2);
+    const double k = div(mul(2., sqr(e)), ope);
     const double t05 = (type == 81) ? div(r.rcut, sub(r.rcut, r.rc)) : 1.0;
-    o.s2 = f32(mul(2., sqe));
-    o.cx1 = f32(cx1);
-    o.icx1 = f32(div(1., cx1));
-    o.cxi = f32(div(1., mul(add(1., e), add(1., e))));
-    o.cyi = f32(div(1., mul(sub(1., e), sub(1., e))));
-    o.ome2 = f32(div(1., sub(1., mul(e, e))));
-    o.e4 = f32(mul(4., e));
-    o.cpi = f32(add(cx1, div(1., cx1)));
-    o.rc = f32(r.rc);
-    o.rcut = f32(r.rcut);
-    o.drs = f32(sub(r.rc, r.rcut));
-    o.dr2 = f32(mul(sub(r.rc, r.rcut), add(r.rc, r.rcut)));
-    o.rc2 = f32(mul(r.rc, r.rc));
-    o.rcut2 = f32(mul(r.rcut, r.rcut));
-    o.s2rc = f32(mul(mul(2., sqe), r.rc));
-    o.s2rcut = f32(mul(mul(2., sqe), r.rcut));
-    o.gpre = f32(mul(mul(mul(0.5, ci), r.b0), t05));
-    o.kpre = f32(type == 81 ? mul(mul(-0.5, r.b0), t05) : mul(0.5, r.b0));
-    o.ppre = f32(mul(mul(ci, r.b0), t05));
-    o.om2 = f32(mul(sub(1., e), sub(1., e)));
-    o.e4cxi = f32(div(mul(4., e), mul(add(1., e), add(1., e))));
-    o.ok3c = f32(mul(mul(sub(1., e), add(3., e)), r.rc));
-    o.ok3t = f32(mul(mul(sub(1., e), add(3., e)), r.rcut));
+    const double A = mul(mul(r.b0, ome), t05), K = mul(0.5, A);
+    const double sc = mul(ope, r.rc), st = mul(ope, r.rcut);
+    const double sc2 = mul(sc, sc), st2 = mul(st, st), ds2 = mul(sub(sc, st), add(sc, st));
+    const double c1 = sub(q2, 1.);
+    o.q2 = f32(q2);
+    o.k = f32(k);
+    o.k2 = f32(mul(k, k));
+    o.sc = f32(sc);
+    o.st = f32(st);
+    o.ds = f32(sub(sc, st));
+    o.dsq2 = f32(mul(q2, sub(sc, st)));
+    o.q2sc2 = f32(mul(q2, sc2));
+    o.q2st2 = f32(mul(q2, st2));
+    o.dq2s2 = f32(mul(q2, ds2));
+    o.opsc2 = f32(mul(opq2, sc2));
+    o.opst2 = f32(mul(opq2, st2));
+    o.opds2 = f32(mul(opq2, ds2));
+    o.tsc = f32(mul(2., sc));
+    o.tst = f32(mul(2., st));
+    o.K = f32(K);
+    o.Kc1sc2 = f32(mul(mul(K, c1), sc2));
+    o.Kc1st2 = f32(mul(mul(K, c1), st2));
+    o.Ak = f32(div(A, k));
+    o.qsc = f32(mul(q, sc));
+    o.qst = f32(mul(q, st));
+    o.q2sc = f32(mul(q2, sc));
+    o.q2st = f32(mul(q2, st));
+    o.Asc = f32(mul(0.5, mul(A, sc)));
+    o.Ast = f32(mul(0.5, mul(A, st)));
     o.i4rc2 = f32(div(1., mul(4., mul(r.rc, r.rc))));
     o.i4rcut2 = f32(div(1., mul(4., mul(r.rcut, r.rcut))));
-    const double sr = type == 81 ? r.rcut : r.rc;
-    o.singv = f32(mul(mul(2., sr), sqe));
-    const double srad = mul(add(kSingFrac, mul(kSingEps, e)), sr);
-    o.sing_r2 = f32(mul(srad, srad));
     const double core_r2 = mul(mul(kCoreFrac, r.rc), mul(kCoreFrac, r.rc));
     /* one radius for both round regions: the near field and the core */
     if (core_r2 > mul(near_r, near_r)) o.rnear2 = f32(core_r2);

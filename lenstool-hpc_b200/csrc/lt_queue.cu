@@ -19,8 +19,8 @@
  *     being rewritten for a later request.
  *   - The tile is evaluated with the same per-chunk pair loops as the single-grid
  *     kernels (lt_eval.cuh), halo chunks staged into shared memory by cp.async.bulk.
- *     FP32C tiles recompute their pixels with |mu| above the flag threshold in FP64
- *     inside the tile, so a request needs no second pass and no pixel list.
+ *     FP32C tiles recompute in FP64, inside the tile, the pixels whose FP32 error bound
+ *     on mu exceeds the tolerance, so a request needs no second pass and no pixel list.
  *   - The CTA that completes the last tile of a request publishes the completion: for
  *     the serving loop a word in mapped host memory set to seq + 1.
  *   - Idle CTAs poll for new requests with __nanosleep for a bounded number of polls and
@@ -199,7 +199,8 @@ __device__ __noinline__ bool tile64(const QItem &it, int tile, Stage &st, int32_
 
 /* FP32C (or, with an all-FP64 chunk list, fast FP64) Hessian/potential sums of one tile:
  * grid32c_kernel's per-tile work followed by the FP64 recomputation of the tile's
- * pixels with |mu| > mu_flag (the single-grid path's second pass, same arithmetic). */
+ * pixels whose FP32 error bound on mu exceeds mu_tol (the single-grid path's second pass,
+ * same arithmetic). */
 template <int OP, int P>
 __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_t *status, int16_t *s_list, int *s_count)
 {
@@ -219,9 +220,15 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
                               if (c.pad & CHUNK_FP32) {
                                   const lt_rec32 *recs = reinterpret_cast<const lt_rec32 *>(buf);
                                   switch (c.type) {
-                                  case 81: eval32_chunk<OP, P, 81>(recs, a.recs, c.count, px, py, a.kmap, acc); break;
-                                  case 8: eval32_chunk<OP, P, 8>(recs, a.recs, c.count, px, py, a.kmap, acc); break;
-                                  case 5: eval32_chunk<OP, P, 5>(recs, a.recs, c.count, px, py, a.kmap, acc); break;
+                                  case 81:
+                                      eval32_chunk<OP, P, 81>(recs, a.recs, c.count, px, py, a, ix, iy, acc);
+                                      break;
+                                  case 8:
+                                      eval32_chunk<OP, P, 8>(recs, a.recs, c.count, px, py, a, ix, iy, acc);
+                                      break;
+                                  case 5:
+                                      eval32_chunk<OP, P, 5>(recs, a.recs, c.count, px, py, a, ix, iy, acc);
+                                      break;
                                   default: break;
                                   }
                               } else {
@@ -235,7 +242,7 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
                               }
                           });
     if (!ok) return false;
-    const bool recompute = (OP & OP_HESS) && it.mu_flag > 0.;
+    const bool recompute = (OP & OP_HESS) && it.mu_tol > 0.;
     if (recompute && threadIdx.x == 0) *s_count = 0;
     if (recompute) __syncthreads();
     if (iy < a.ny) {
@@ -244,10 +251,10 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
         bool flag[P];
 #pragma unroll
         for (int k = 0; k < P; k++) {
-            double det;
-            fp32c_total(acc, k, a.D, hxx[k], hyy[k], hxy[k], psi[k], det);
+            double det, det_err;
+            fp32c_total(acc, k, a.D, hxx[k], hyy[k], hxy[k], psi[k], det, det_err);
             fp32c_grad_total(acc, k, gx[k], gy[k]);
-            flag[k] = recompute && !(fabs(det) * it.mu_flag >= 1.0);
+            flag[k] = recompute && fp32c_flag(det, det_err, it.mu_tol);
         }
         const bool full = a.vec_ok && (ix + P <= a.nx);
         for (int o = 0; o < a.nout; o++) {
@@ -314,10 +321,11 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
 }
 
 /* Claim one tile (thread 0).  Returns 1 with (slot, tile) set, 0 when no published
- * request has tiles left.  Every attempt either claims a tile or finds the head request
- * exhausted and moves the head on (here or in another CTA), so the attempts are bounded
- * by the published requests; the limit below is only a safety net. */
-__device__ int claim_tile(const QArgs &q, int &slot_out, int &tile_out)
+ * request has tiles left, 2 when none has and the oldest published request's descriptor
+ * has not arrived (its seq in *missing).  Every attempt either claims a tile or finds the
+ * head request exhausted and moves the head on (here or in another CTA), so the attempts
+ * are bounded by the published requests; the limit below is only a safety net. */
+__device__ int claim_tile(const QArgs &q, int &slot_out, int &tile_out, uint32_t *missing)
 {
     QState *st = q.state;
     for (int attempt = 0; attempt < (1 << 20); attempt++) {
@@ -327,7 +335,7 @@ __device__ int claim_tile(const QArgs &q, int &slot_out, int &tile_out)
         unsigned long long span = p - h;
         if (span > (unsigned long long)q.window) span = (unsigned long long)q.window;
         const unsigned long long r0 = atomicAdd(&st->rotor, 1ull);
-        bool head_exhausted = false;
+        bool head_exhausted = false, head_missing = false;
         for (unsigned long long k = 0; k < span; k++) {
             const unsigned long long r = h + (r0 + k) % span;
             QSlot *s = q.slots + (r % (unsigned long long)q.nslots);
@@ -348,16 +356,22 @@ __device__ int claim_tile(const QArgs &q, int &slot_out, int &tile_out)
              * not received r's descriptor yet: r is not exhausted. */
             const int32_t age = (int32_t)((uint32_t)(c >> 32) - (uint32_t)r);
             if (r == h && age >= 0) head_exhausted = true;
+            if (r == h && (age < 0 || seq != (uint32_t)r)) head_missing = true;
         }
         /* the head request has no tiles left (or its slot already holds a later
          * request): move the head on */
-        if (head_exhausted) atomicCAS(&st->head, h, h + 1ull);
+        if (head_exhausted) {
+            atomicCAS(&st->head, h, h + 1ull);
+        } else if (head_missing) {
+            *missing = (uint32_t)h;
+            return 2;
+        }
     }
     return 0;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kQThreads, 2) queue_kernel(const QArgs q)
+template <int MODE, int P32, int MINB>
+__global__ void __launch_bounds__(kQThreads, MINB) queue_kernel(const QArgs q)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
@@ -381,13 +395,31 @@ __global__ void __launch_bounds__(kQThreads, 2) queue_kernel(const QArgs q)
         if (tid == 0) {
             int slot = -1, tile = 0;
             bool counted = false; /* this CTA is in QState::idle */
+            int missing_polls = 0;
             for (int polls = 0;; polls++) {
                 if (*(volatile int32_t *)&q.state->yield) break;
-                if (claim_tile(q, slot, tile)) {
+                uint32_t missing = 0;
+                const int got = claim_tile(q, slot, tile, &missing);
+                if (got == 1) {
                     if (counted) atomicSub(&q.state->idle, 1);
                     break;
                 }
                 slot = -1;
+                /* a published request whose descriptor does not arrive: a bounded wait (not
+                 * an idle poll: the launch does not leave on idle meanwhile), then the
+                 * request is reported (its seq + 1 in QState::stuck, the status word
+                 * LT_ERR_TIMEOUT) and the launch leaves */
+                if (got == 2) {
+                    if (++missing_polls > q.desc_polls) {
+                        atomicExch(&q.state->stuck, missing + 1u);
+                        if (q.status) atomicExch(q.status, (int32_t)LT_ERR_TIMEOUT);
+                        atomicExch(&q.state->yield, 1);
+                        break;
+                    }
+                    __nanosleep(1000);
+                    continue;
+                }
+                missing_polls = 0;
                 if (*(volatile int32_t *)&q.state->stop) break;
                 if (!counted) {
                     atomicAdd(&q.state->idle, 1);
@@ -416,11 +448,11 @@ __global__ void __launch_bounds__(kQThreads, 2) queue_kernel(const QArgs q)
         bool ok = true;
         const int hp = item.op & (OP_HESS | OP_POT);
         if (MODE == QMODE_C32) {
-            if (item.op & OP_GRAD) ok = tile32<OP_GRAD, 2>(item, tile, st, q.status, s_list, &s_count);
-            if (ok && hp == OP_HESS) ok = tile32<OP_HESS, 2>(item, tile, st, q.status, s_list, &s_count);
-            if (ok && hp == OP_POT) ok = tile32<OP_POT, 2>(item, tile, st, q.status, s_list, &s_count);
+            if (item.op & OP_GRAD) ok = tile32<OP_GRAD, P32>(item, tile, st, q.status, s_list, &s_count);
+            if (ok && hp == OP_HESS) ok = tile32<OP_HESS, P32>(item, tile, st, q.status, s_list, &s_count);
+            if (ok && hp == OP_POT) ok = tile32<OP_POT, P32>(item, tile, st, q.status, s_list, &s_count);
             if (ok && hp == (OP_HESS | OP_POT))
-                ok = tile32<OP_HESS | OP_POT, 2>(item, tile, st, q.status, s_list, &s_count);
+                ok = tile32<OP_HESS | OP_POT, P32>(item, tile, st, q.status, s_list, &s_count);
         } else if (item.ppt == 2) { /* requests without the potential */
             if (item.op & OP_GRAD) ok = tile64<OP_GRAD, 2>(item, tile, st, q.status);
             if (ok && hp == OP_HESS) ok = tile64<OP_HEX, 2>(item, tile, st, q.status);
@@ -464,25 +496,41 @@ __global__ void queue_reset_kernel(QSlot *slots, QState *state, int n)
 
 /* ------------------------------------------------------------------- host ---- */
 
-int queue_blocks(int mode, int num_sms)
+using QKern = void (*)(const QArgs);
+
+static QKern queue_kernel_for(int mode, int variant)
+{
+    if (mode != QMODE_C32) return queue_kernel<QMODE_EXACT, 2, 2>;
+    switch (variant) {
+    case LT_SHAPE(1, 1): return queue_kernel<QMODE_C32, 1, 1>;
+    case LT_SHAPE(1, 2): return queue_kernel<QMODE_C32, 1, 2>;
+    case LT_SHAPE(2, 1): return queue_kernel<QMODE_C32, 2, 1>;
+    default: return queue_kernel<QMODE_C32, 2, 2>;
+    }
+}
+
+/* The built variant nearest to an FP32C grid-kernel shape: its pixels per thread, and its
+ * resident threads per SM rounded to 256 or 512. */
+int queue_variant(int shape32)
+{
+    const int ppt = shape_ppt(shape32) == 1 ? 1 : 2;
+    const int threads = shape_cps(shape32) * shape_threads(shape32);
+    return LT_SHAPE(ppt, threads > 384 ? 2 : 1);
+}
+
+int queue_blocks(int mode, int variant, int num_sms)
 {
     const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
     int per_sm = 0;
-    if (mode == QMODE_C32)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, queue_kernel<QMODE_C32>, kQThreads, smem);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, queue_kernel<QMODE_EXACT>, kQThreads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, queue_kernel_for(mode, variant), kQThreads, smem);
     if (per_sm < 1) per_sm = 1;
     return per_sm * num_sms;
 }
 
-int launch_queue(int mode, const QArgs &q, int blocks, cudaStream_t s)
+int launch_queue(int mode, int variant, const QArgs &q, int blocks, cudaStream_t s)
 {
     const size_t smem = 2 * LT_CHUNK * sizeof(lt_rec64);
-    if (mode == QMODE_C32)
-        queue_kernel<QMODE_C32><<<blocks, kQThreads, smem, s>>>(q);
-    else
-        queue_kernel<QMODE_EXACT><<<blocks, kQThreads, smem, s>>>(q);
+    queue_kernel_for(mode, variant)<<<blocks, kQThreads, smem, s>>>(q);
     return (int)cudaGetLastError();
 }
 

@@ -30,7 +30,8 @@ struct alignas(16) QItem {
     uint32_t seq;               /* request sequence number (low 32 bits) */
     int32_t ppt;                /* pixels per thread of the tiles (QMODE_EXACT) */
     int32_t pad0;
-    double mu_flag;             /* FP32C: recompute pixels with |mu| > mu_flag in FP64 */
+    double mu_tol;              /* FP32C: recompute pixels whose FP32 error bound on mu exceeds
+                                   this in FP64 (0: none) */
     uint32_t *host_flag;        /* mapped host word set to seq + 1 on completion, or null */
     int64_t pad1;
 };
@@ -50,7 +51,7 @@ struct alignas(16) QState {
     int32_t stop;                  /* leave when no published request has work */
     int32_t yield;                 /* leave at the next claim; unclaimed tiles stay for the next launch */
     int32_t idle;                  /* CTAs of the running launch without work (or gone) */
-    int32_t pad;
+    uint32_t stuck;                /* seq + 1 of a published request whose descriptor never came */
 };
 
 struct QArgs {
@@ -59,11 +60,17 @@ struct QArgs {
     int32_t nslots;
     int32_t window;                /* requests served round-robin (1: first come, first served) */
     int32_t idle_polls;            /* polls of ~1 us before an idle CTA leaves */
+    int32_t desc_polls;            /* polls of ~1 us a CTA waits for the descriptor of the oldest
+                                      published request before reporting LT_ERR_TIMEOUT */
     int32_t *status;               /* device status word (LT_ERR_TIMEOUT from a bounded wait) */
 };
 
-int queue_blocks(int mode, int num_sms);
-int launch_queue(int mode, const QArgs &q, int blocks, cudaStream_t s);
+/* Persistent-kernel variants: the FP32C tiles come with 1 or 2 pixels per thread and
+ * registers cut for 1 or 2 resident CTAs per SM (256 threads); `variant` is their
+ * LT_SHAPE(pixels, CTAs).  The LT_FP64 tiles have one variant (2 CTAs per SM). */
+int queue_variant(int shape32);
+int queue_blocks(int mode, int variant, int num_sms);
+int launch_queue(int mode, int variant, const QArgs &q, int blocks, cudaStream_t s);
 int launch_queue_reset(QSlot *slots, QState *state, int n, cudaStream_t s);
 
 } // namespace lt

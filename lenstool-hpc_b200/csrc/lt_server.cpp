@@ -43,7 +43,8 @@
 using namespace lt;
 
 namespace lt {
-lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, double *const *outs, QItem *it);
+lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, double *const *outs, QItem *it,
+                          int ppt32);
 void free_catalog(lt_context *ctx, lt_catalog *cat);
 
 /* Context-level state of the serving extension: catalogues released while a server
@@ -125,7 +126,9 @@ double ms_between(Clock::time_point a, Clock::time_point b)
 struct lt_server {
     lt_context *ctx = nullptr;
     int precision = LT_FP32C, mode = QMODE_C32;
-    int nslots = 64, window = 8, idle_polls = 20000, blocks = 0;
+    int nslots = 64, window = 8, idle_polls = 20000, desc_polls = 2000000, blocks = 0;
+    int variant = LT_SHAPE(2, 2);        /* queue kernel variant (FP32C: pixels, CTAs per SM) */
+    bool drop_next = false;              /* fault injection: publish the next request without its descriptor */
     QSlot *slots = nullptr;
     QState *state = nullptr;
     size_t dev_bytes = 0, arena_bytes = 0;
@@ -214,7 +217,7 @@ void admit(lt_server *s)
         }
         QSlot &hs = s->h_slots[slot];
         memset(&hs, 0, sizeof(hs));
-        lt_status st = make_queue_item(s->ctx, &r->req, s->precision, outs, &hs.item);
+        lt_status st = make_queue_item(s->ctx, &r->req, s->precision, outs, &hs.item, shape_ppt(s->variant));
         s->pending.pop_front();
         if (st != LT_OK) {
             finish(s, r, st);
@@ -228,7 +231,10 @@ void admit(lt_server *s)
         hs.done = 0u;
         __atomic_store_n(&s->h_flags[slot], 0u, __ATOMIC_RELEASE);
         s->h_pub[slot] = seq + 1;
-        cudaMemcpyAsync(&s->slots[slot], &hs, sizeof(QSlot), cudaMemcpyHostToDevice, s->pub_stream);
+        if (s->drop_next) /* injected fault: the descriptor is lost, the request still published */
+            s->drop_next = false;
+        else
+            cudaMemcpyAsync(&s->slots[slot], &hs, sizeof(QSlot), cudaMemcpyHostToDevice, s->pub_stream);
         cudaMemcpyAsync(&s->state->published, &s->h_pub[slot], sizeof(unsigned long long), cudaMemcpyHostToDevice,
                         s->pub_stream);
         r->slot = slot;
@@ -342,6 +348,34 @@ void run_tails(lt_server *s)
     }
 }
 
+/* The loop reported a published request whose descriptor never reached the device
+ * (QState::stuck = its seq + 1): fail that request with LT_ERR_TIMEOUT, put an empty
+ * descriptor of its seq in its slot so the device's head moves past it, and clear the
+ * report.  Returns false when no running request has that seq. */
+bool drop_stuck(lt_server *s)
+{
+    const uint32_t seq = (uint32_t)s->h_status[1] - 1u;
+    for (int slot = 0; slot < s->nslots; slot++) {
+        SrvReq *r = s->ring[slot];
+        if (!r || r->state != R_RUNNING || (uint32_t)r->seq != seq) continue;
+        QSlot &hs = s->h_slots[slot];
+        memset(&hs, 0, sizeof(hs));
+        hs.item.seq = seq;
+        hs.item.ntiles = 0;
+        hs.ctr = (unsigned long long)seq << 32;
+        cudaMemcpyAsync(&s->slots[slot], &hs, sizeof(QSlot), cudaMemcpyHostToDevice, s->pub_stream);
+        cudaMemsetAsync(&s->state->stuck, 0, sizeof(uint32_t), s->pub_stream);
+        cudaMemsetAsync(s->ctx->status, 0, sizeof(int32_t), s->pub_stream);
+        set_error(s->ctx, "request %llu: its descriptor did not reach the device within the wait limit",
+                  (unsigned long long)r->ticket);
+        finish(s, r, LT_ERR_TIMEOUT);
+        s->stats.timed_out++;
+        s->cv_done.notify_all();
+        return true;
+    }
+    return false;
+}
+
 /* Keep the persistent kernel running while requests are in flight. */
 void keep_loop(lt_server *s)
 {
@@ -354,7 +388,10 @@ void keep_loop(lt_server *s)
         if (e == cudaErrorNotReady) return;
         /* the kernel has left: was it a bounded wait that gave up? */
         cudaMemcpyAsync(s->h_status, s->ctx->status, sizeof(int32_t), cudaMemcpyDeviceToHost, s->pub_stream);
+        cudaMemcpyAsync(s->h_status + 1, &s->state->stuck, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->pub_stream);
         cudaStreamSynchronize(s->pub_stream);
+        if (e == cudaSuccess && *s->h_status == LT_ERR_TIMEOUT && s->h_status[1] != 0 && drop_stuck(s))
+            return; /* relaunched at the next pass, without the request */
         if (e != cudaSuccess || *s->h_status != 0) {
             const lt_status st = e != cudaSuccess ? LT_ERR_CUDA : (lt_status)*s->h_status;
             set_error(s->ctx, "serving loop kernel stopped: %s",
@@ -376,6 +413,7 @@ void keep_loop(lt_server *s)
     q.nslots = s->nslots;
     q.window = s->window;
     q.idle_polls = s->idle_polls;
+    q.desc_polls = s->desc_polls;
     q.status = s->ctx->status;
     /* a new launch starts with no CTA idle and no yield pending (the last launch may have
      * left together on idle, setting yield from the device) */
@@ -386,7 +424,7 @@ void keep_loop(lt_server *s)
     cudaEventRecord(pub, s->pub_stream);
     cudaStreamWaitEvent(s->loop_stream, pub, 0);
     cudaEventDestroy(pub);
-    const int err = launch_queue(s->mode, q, s->blocks, s->loop_stream);
+    const int err = launch_queue(s->mode, s->variant, q, s->blocks, s->loop_stream);
     count_launch(1);
     cudaEventRecord(s->loop_done, s->loop_stream);
     s->loop_launched = true;
@@ -445,7 +483,7 @@ lt_status lt_server_create(lt_context *ctx, const lt_server_config *cfg, lt_serv
         set_error(ctx, "the serving loop runs LT_FP32C or LT_FP64");
         return LT_ERR_INVALID_ARGUMENT;
     }
-    if (c.slots < 0 || c.window < 0 || c.idle_us < 0) return LT_ERR_INVALID_ARGUMENT;
+    if (c.slots < 0 || c.window < 0 || c.idle_us < 0 || c.descriptor_wait_us < 0) return LT_ERR_INVALID_ARGUMENT;
     lt_server *s = new (std::nothrow) lt_server();
     if (!s) return LT_ERR_OUT_OF_MEMORY;
     s->ctx = ctx;
@@ -454,6 +492,7 @@ lt_status lt_server_create(lt_context *ctx, const lt_server_config *cfg, lt_serv
     s->nslots = c.slots ? c.slots : 64;
     s->window = std::min(c.window ? c.window : 8, s->nslots);
     s->idle_polls = c.idle_us ? c.idle_us : 20000;
+    s->desc_polls = c.descriptor_wait_us > 0 ? c.descriptor_wait_us : 2000000;
     const size_t arena_bytes = c.output_bytes ? c.output_bytes : ((size_t)4 << 30);
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
@@ -500,12 +539,38 @@ lt_status lt_server_create(lt_context *ctx, const lt_server_config *cfg, lt_serv
         delete s;
         return cuda_fail(ctx, e, "server setup");
     }
+    /* every slot starts out showing request seq 2^32 - 1 (an "earlier" request for the
+     * first ones), so a slot whose descriptor has not arrived never reads as request 0 */
+    memset(s->h_slots, 0, sizeof(QSlot) * (size_t)s->nslots);
+    for (int i = 0; i < s->nslots; i++) {
+        s->h_slots[i].item.seq = 0xffffffffu;
+        s->h_slots[i].ctr = 0xffffffffull << 32;
+    }
+    e = cudaMemcpy(s->slots, s->h_slots, sizeof(QSlot) * (size_t)s->nslots, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        /* the same clean-up as above, after which every buffer is allocated */
+        cudaFreeHost(s->h_slots);
+        cudaFreeHost(s->h_pub);
+        cudaFreeHost(s->h_status);
+        cudaFreeHost(s->h_chi);
+        cudaFreeHost(s->h_yield);
+        cudaFreeHost(s->h_flags);
+        cudaStreamDestroy(s->loop_stream);
+        cudaStreamDestroy(s->pub_stream);
+        cudaStreamDestroy(s->copy_stream);
+        cudaEventDestroy(s->loop_done);
+        dev_free(ctx, s->arena_mem, arena_bytes);
+        dev_free(ctx, mem, s->dev_bytes);
+        delete s;
+        return cuda_fail(ctx, e, "server setup");
+    }
     memset(s->h_flags, 0, sizeof(uint32_t) * (size_t)s->nslots);
     memset(s->h_chi, 0, 2 * sizeof(double) * (size_t)s->nslots);
     s->h_yield[0] = 1;
     s->h_yield[1] = 0;
     s->ring.assign((size_t)s->nslots, nullptr);
-    s->blocks = queue_blocks(s->mode, ctx->num_sms);
+    s->variant = queue_variant(ctx->shape[LT_FP32C][OP_HESS]);
+    s->blocks = queue_blocks(s->mode, s->variant, ctx->num_sms);
     {
         Extensions *x = ext_of(ctx);
         std::lock_guard<std::mutex> xl(x->mu);
@@ -531,7 +596,7 @@ lt_status lt_server_submit(lt_server *s, const lt_request *req, uint64_t *ticket
     double *probe[LT_MAX_MAPS];
     for (int i = 0; i < LT_MAX_MAPS; i++) probe[i] = (double *)s->arena_mem;
     QItem tmp;
-    lt_status st = make_queue_item(s->ctx, req, s->precision, host ? probe : nullptr, &tmp);
+    lt_status st = make_queue_item(s->ctx, req, s->precision, host ? probe : nullptr, &tmp, shape_ppt(s->variant));
     if (st == LT_OK && host)
         for (int i = 0; i < req->nmaps; i++)
             if (!req->maps[i].out) st = LT_ERR_INVALID_ARGUMENT;
@@ -611,7 +676,7 @@ lt_status lt_server_submit_chi2(lt_server *s, const lt_catalog *cat, const lt_fr
     double *probe[LT_MAX_MAPS];
     for (int i = 0; i < LT_MAX_MAPS; i++) probe[i] = (double *)s->arena_mem;
     QItem tmp;
-    st = make_queue_item(ctx, &g, s->precision, probe, &tmp);
+    st = make_queue_item(ctx, &g, s->precision, probe, &tmp, shape_ppt(s->variant));
     if (st == LT_OK && r->chi_bytes > s->arena.size()) {
         set_error(ctx, "chi2 request needs %zu bytes; the server's arena holds %zu", r->chi_bytes, s->arena.size());
         st = LT_ERR_BUDGET;
@@ -729,6 +794,14 @@ lt_status lt_server_get_stats(lt_server *s, lt_server_stats *out)
         out->device_published = hq->published;
         out->device_head = hq->head;
     }
+    return LT_OK;
+}
+
+lt_status lt_server_inject_fault(lt_server *s, int32_t fault)
+{
+    if (!s || fault != LT_FAULT_DROP_DESCRIPTOR) return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(s->mu);
+    s->drop_next = true;
     return LT_OK;
 }
 

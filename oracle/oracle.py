@@ -21,7 +21,17 @@ HERE = pathlib.Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liblt_oracle.so"
 ORACLE_LD_SO = HERE / "liblt_oracle_ld.so"
 REF_SO = HERE / "_ref" / "libltref.so"
-REFERENCE_TREE = pathlib.Path("/root/reference")
+
+
+def reference_tree() -> pathlib.Path:
+    """The reference source tree the checker library is built from: $LT_REFERENCE_TREE,
+    else the default of the build recipe (oracle/Makefile, variable REF)."""
+    env = os.environ.get("LT_REFERENCE_TREE")
+    if env:
+        return pathlib.Path(env)
+    r = subprocess.run(["make", "-s", "--no-print-directory", "print-ref"], cwd=HERE, capture_output=True, text=True)
+    return pathlib.Path(r.stdout.strip() or ".")
+
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -30,10 +40,11 @@ _ip = C.POINTER(C.c_int)
 def build(with_reference: bool | None = None) -> None:
     """Compile the oracle, and the reference library when the reference tree exists."""
     subprocess.run(["make", "-s", "oracle"], cwd=HERE, check=True)
+    tree = reference_tree()
     if with_reference is None:
-        with_reference = (REFERENCE_TREE / "src" / "gradient.cpp").exists()
+        with_reference = (tree / "src" / "gradient.cpp").exists()
     if with_reference:
-        subprocess.run(["make", "-s", "ref", f"REF={REFERENCE_TREE}"], cwd=HERE, check=True)
+        subprocess.run(["make", "-s", "ref", f"REF={tree}"], cwd=HERE, check=True)
 
 
 def _d(a):
@@ -315,12 +326,16 @@ class RefLib:
         return {k: out[:, i, :] for i, k in enumerate(keys)}
 
 
-REF_GPU_SO = {"fp64": HERE / "_ref" / "libltref_gpu.so", "fp32": HERE / "_ref" / "libltref_gpu32.so"}
+REF_GPU_SO = {"fp64": HERE / "_ref" / "libltref_gpu.so", "fp32": HERE / "_ref" / "libltref_gpu32.so",
+              "fp64_stock": HERE / "_ref" / "libltref_gpu_stock.so",
+              "fp32_stock": HERE / "_ref" / "libltref_gpu32_stock.so"}
 
 
 class RefGpuLib:
     """The reference's own GPU kernels (src/gradient2_GPU.cu, src/potential_GPU.cu) built
-    for sm_100a: type_t = double ("fp64") or float ("fp32", the reference's default)."""
+    for sm_100a: "fp64_stock" with the flags of its default build (-O3 -use_fast_math,
+    type_t = double), "fp32_stock" the same with type_t = float, and "fp64" / "fp32"
+    with -O3 alone."""
 
     def __init__(self, build="fp64"):
         path = REF_GPU_SO[build]

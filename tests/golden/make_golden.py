@@ -14,13 +14,15 @@ committed so the GPU tests never read the reference tree.
                    (gradient2_grid_CPU), amplif_grid_CPU mode 5, the GPU Hessian and Kmap
                    kernels and the potential kernel (run on the host) for the dPIE file.
 
-Usage:  python tests/golden/make_golden.py [--reference /root/reference]
+Usage:  python tests/golden/make_golden.py --reference <reference tree>
+        (or with the tree in $LT_REFERENCE_TREE)
 """
 from __future__ import annotations
 
 import argparse
 import importlib.util
 import math
+import os
 import pathlib
 import re
 import sys
@@ -161,8 +163,12 @@ def par_fixture(ref_tree, out, name, catalog, reflib, n=33):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("LT_REFERENCE_TREE"),
+                    help="the reference source tree (default: $LT_REFERENCE_TREE)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference or set LT_REFERENCE_TREE")
+    os.environ["LT_REFERENCE_TREE"] = args.reference
     ref_tree = pathlib.Path(args.reference)
     pkg = _load_pkg()
     from lenstool_hpc_b200 import catalog  # noqa: E402

@@ -180,3 +180,51 @@ def test_batch_rejects_bad_requests(ctx):
     assert e.value.status == 1
     with pytest.raises(lt.LensError):
         ctx.batch([lt.Request(cat, g, {99: _dev(g)})])
+
+
+def test_autotune_shape_is_applied_to_batches():
+    """lt_autotune searches the FP32C configurations (pixels per thread, CTAs per SM,
+    threads per CTA, halo records per stage) on a grid over the catalogue and keeps the
+    fastest; the maps in the tuned configuration stay within 1e-6 of LT_FP64, and a batch
+    built afterwards runs its persistent kernel with the tuned pixels per thread (its
+    lt_batch_config) and equals the single calls in that configuration bit for bit."""
+    import torch
+    from conftest import max_rel_err
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lenstool_hpc_b200 import build
+    build.build()
+    c = lt.Context(0)
+    try:
+        cat = c.upload(catalog.cluster_galaxy_catalog(2, 198, 20261203))
+        default = c.kernel_config("fp32c", "hessian")
+        ppt, cps, ms = c.autotune(cat, "fp32c", "hessian", grid_n=384)
+        cfg = c.kernel_config("fp32c", "hessian")
+        assert ms > 0 and (ppt, cps) == (cfg["pixels_per_thread"], cfg["ctas_per_sm"])
+        assert cfg["threads"] in (128, 256) and cfg["chunk"] in (32, 64, 128)
+        print("default", default, "tuned", cfg, f"{ms:.3f} ms")
+        g = catalog.Grid(-100., 100., -100., 100., 300, 260)
+        kinds = ["kappa", "gamma1", "mu"]
+        tuned = _single(c, cat, g, kinds, {}, "fp32c", D=0.62)
+        ref = _single(c, cat, g, kinds, {}, "fp64", D=0.62)
+        mask = np.abs(ref["mu"]) <= 100
+        for k in kinds:
+            assert max_rel_err(tuned[k], ref[k], mask) <= 1e-6, k
+        outs = {k: _dev(g) for k in kinds}
+        b = c.batch([lt.Request(cat, g, outs, dlsds=0.62)], precision="fp32c")
+        bc = b.config()
+        assert bc["pixels_per_thread"] == cfg["pixels_per_thread"]
+        b.launch()
+        c.synchronize()
+        torch.cuda.synchronize()
+        for k in kinds:
+            assert np.array_equal(outs[k].cpu().numpy(), tuned[k]), k
+        b.destroy()
+        # every built configuration can be set; unbuilt ones are refused
+        c.set_kernel_config("fp32c", "hessian", 2, 3, 128, 32)
+        with pytest.raises(lt.LensError):
+            c.set_kernel_config("fp32c", "hessian", 2, 3, 256, 64)
+        with pytest.raises(lt.LensError):
+            c.set_kernel_config("fp64", "hessian", 2, 2, 128, 64)
+    finally:
+        c.close()

@@ -43,18 +43,30 @@ def _maps(ctx, cat, g, precision, D=0.6, kinds=("kappa", "gamma1", "gamma2", "mu
 
 
 def test_fp32c_workload_maps(ctx):
-    """The 1000-halo 4096^2 workload: kappa, gamma1, gamma2, mu within 1e-6."""
+    """The 1000-halo 4096^2 workload through the fused lens-maps call (the benchmarked
+    step): kappa, gamma1, gamma2, mu and psi of LT_FP32C within 1e-6 of LT_FP64 (whose
+    Hessian equals the reference's CPU arithmetic bit for bit and whose potential is the
+    reference's pi05), pixels with |mu| > 100 reported on their own."""
+    import torch
+    from lenstool_hpc_b200.accuracy import map_errors
     cat, g = catalog.workload("maps_1000h_4096")
+    dls, dos, _ = lt.cosmo_distances(0.35, 1.5)
+    D = dls / dos  # lens at z 0.35, sources at z 1.5, as in the benchmark
     dcat = ctx.upload(cat)
-    m64 = _maps(ctx, dcat, g, "fp64")
-    m32 = _maps(ctx, dcat, g, "fp32c")
-    mask = np.isfinite(m64["mu"]) & (np.abs(m64["mu"]) <= 100)
-    errs = {k: rel_errors(m32[k], m64[k], mask) for k in m64}
-    high = ~mask & np.isfinite(m64["mu"])
-    errs_high = {k: rel_errors(m32[k], m64[k], high) for k in ("kappa", "gamma1", "gamma2")} if high.any() else {}
-    print("fp32c max rel err (|mu|<=100):", errs, " |mu|>100 pixels:", int(high.sum()), errs_high)
+    names = ("kappa", "gamma1", "gamma2", "mu", "psi")
+    res = {}
+    for prec in ("fp64", "fp32c"):
+        res[prec] = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in names}
+        ctx.lens_maps(dcat, g, precision=prec, dlsds=D, out=res[prec])
+        ctx.synchronize()
+    errs = map_errors(res["fp32c"], res["fp64"])
     for k, e in errs.items():
-        assert e <= TOL32, (k, e)
+        print(f"fp32c {k}: max {e['max']:.3e} rms {e['rms']:.3e} over {e['pixels']} px; |mu|>100: "
+              f"max {e['max_mu_gt_cut']:.3e} rms {e['rms_mu_gt_cut']:.3e} over {e['pixels_mu_gt_cut']} px")
+    for k in names:
+        assert errs[k]["max"] <= TOL32, (k, errs[k])
+    # the excluded pixels are few: the critical curves of a 4096^2 map
+    assert errs["mu"]["pixels_mu_gt_cut"] < 1e-2 * g.npix
 
 
 @pytest.mark.parametrize("cluster_type", [81, 8, 5])

@@ -156,12 +156,20 @@ def test_every_map_kind_vs_oracle(ctx, oracle_lib):
     kinds = ["ampli1", "ampli2", "ampli3", "ampli4", "ampli5", "ampli6", "shear1", "shear2"]
     m = ctx.hessian_maps(cat, g, kinds, dlsds=D)
     for k in kinds:
-        assert max_rel_err(m[k], oracle_lib.map(k, a, b, c, D).reshape(g.ny, g.nx)) <= 1e-10, k
+        ref = oracle_lib.map(k, a, b, c, D).reshape(g.ny, g.nx)
+        if k == "ampli3":
+            # -2.5 log10|det|: CUDA's log10 and the C library's are each within a couple
+            # of ulp of the exact value, so the two agree to a few ulp of the result
+            assert max_rel_err(m[k], ref) <= TOL, k
+        else:
+            # every other kind is +, -, *, / and sqrt, correctly rounded on both sides, in
+            # the reference's operation order on identical Hessian planes
+            assert np.array_equal(m[k], ref), (k, max_rel_err(m[k], ref))
     kinds = ["shear3", "shear4", "kappa", "gamma1", "gamma2", "mu", "mass"]
     m = ctx.hessian_maps(cat, g, kinds, dlsds=D, mult=3.5)
     for k in kinds:
         ref = oracle_lib.map("scale" if k == "mass" else k, a, b, c, D, 3.5).reshape(g.ny, g.nx)
-        assert max_rel_err(m[k], ref) <= 1e-10, k
+        assert np.array_equal(m[k], ref), (k, max_rel_err(m[k], ref))
 
 
 def test_lens_maps_fused_equals_separate(ctx, oracle_lib):
@@ -171,8 +179,29 @@ def test_lens_maps_fused_equals_separate(ctx, oracle_lib):
     out = ctx.lens_maps(cat, g, dlsds=D)
     a, b, c, d = oracle_lib.hess_grid(cat, g)
     for k in ("kappa", "gamma1", "gamma2", "mu"):
-        assert max_rel_err(out[k], oracle_lib.map(k, a, b, c, D).reshape(g.ny, g.nx)) <= 1e-10, k
+        ref = oracle_lib.map(k, a, b, c, D).reshape(g.ny, g.nx)
+        assert np.array_equal(out[k], ref), (k, max_rel_err(out[k], ref))
     assert max_rel_err(out["psi"], D * oracle_lib.pot_grid(cat, g)) <= TOL
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp64fast"])
+def test_c0_gradient_full_grid_vs_reference(ctx, ref_lib, precision):
+    """The plain FP64 deflection workload at its own size: 200 halos (2 PIEMD cluster
+    halos + 198 cut-dPIE galaxies) on the full 1024^2 grid over 200"x200", against the
+    reference's own gradient_grid_CPU (src/grid_gradient_CPU.cpp:33-100, compiled from its
+    sources) at 1e-12 of max(|ref|, RMS) on every pixel."""
+    import torch
+    cat, g = catalog.workload("grad_200h_1024")
+    assert (cat.n, g.nx, g.ny) == (200, 1024, 1024)
+    ax = torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda")
+    ay = torch.empty_like(ax)
+    ctx.gradient_grid(cat, g, precision=precision, out=(ax, ay))
+    ctx.synchronize()
+    rx, ry = ref_lib.grad_grid(cat, g)
+    ex = max_rel_err(ax.cpu().numpy(), rx)
+    ey = max_rel_err(ay.cpu().numpy(), ry)
+    print(f"C0 {precision}: max rel err alpha_x {ex:.3e} alpha_y {ey:.3e}")
+    assert ex <= TOL and ey <= TOL
 
 
 def test_device_outputs_and_stream(ctx, oracle_lib):

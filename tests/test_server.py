@@ -197,3 +197,38 @@ def test_server_chi2_requests_in_a_mix(ctx, precision):
                 assert plane_close(v.cpu().numpy(), exp[k], k, precision), (precision, i, k)
         with pytest.raises(lt.LensError):
             srv.chi2_result(map_t[0])  # not a chi2 ticket
+
+
+def test_lost_descriptor_times_out_and_the_loop_serves_on(ctx):
+    """Failure injection on the host: the next admitted request is published without its
+    descriptor (a lost message).  The loop's bounded wait for it runs out on the device
+    (a 50 ms limit here), the request fails with LT_ERR_TIMEOUT through the C ABI, and the
+    requests submitted before and after it complete with the results of the single-grid
+    calls.  No trap, no unbounded wait: the kernel reports and leaves, the host relaunches."""
+    import torch
+    cat = ctx.upload(catalog.cluster_galaxy_catalog(1, 60, 17))
+    g = catalog.Grid.square(60., 256)
+    D = 0.6
+    want = _alone(ctx, cat, g, ["kappa", "mu"], "fp32c", D, 1.0)
+    dev = lambda: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda")  # noqa: E731
+    with ctx.server(precision="fp32c", slots=8, window=4, descriptor_wait_us=50000) as srv:
+        before = {"kappa": dev(), "mu": dev()}
+        tb = srv.submit(lt.Request(cat, g, before, dlsds=D))
+        srv.wait(tb, 60.)
+        srv.inject_fault(1)
+        lost = srv.submit(lt.Request(cat, g, {"kappa": dev(), "mu": dev()}, dlsds=D))
+        with pytest.raises(lt.LensError) as e:
+            srv.wait(lost, 60.)
+        assert e.value.status == 8  # LT_ERR_TIMEOUT
+        after = [{"kappa": dev(), "mu": dev()} for _ in range(3)]
+        tickets = [srv.submit(lt.Request(cat, g, o, dlsds=D)) for o in after]
+        for t in tickets:
+            srv.wait(t, 60.)
+        st = srv.stats()
+        assert st["timed_out"] == 1 and st["failed"] == 1 and st["completed"] == 4
+    for o in [before] + after:
+        for k in ("kappa", "mu"):
+            assert plane_close(o[k].cpu().numpy(), want[k], k, "fp32c"), k
+    # the context is usable afterwards
+    m = ctx.hessian_maps(cat, g, ["kappa", "mu"], precision="fp32c", dlsds=D)
+    assert np.array_equal(m["kappa"], want["kappa"]) and np.array_equal(m["mu"], want["mu"])

@@ -61,6 +61,53 @@ def test_noalloc_matches_hessian_maps_twice(env):
             assert max_rel_err(got, ref[k]) <= TOL, (call, k)
 
 
+def test_noalloc_allocates_nothing_and_uses_its_list(env):
+    """On a warmed context, repeated calls leave the device's free memory unchanged, and
+    the grid has pixels near critical curves (|mu| > 100, always recomputed in FP64), so
+    the equality with lt_hessian_maps shows the static list at work."""
+    import torch
+    ctx, fn = env
+    cat, _ = catalog.workload("maps_1000h_4096")
+    g = catalog.Grid.square(150., 1024)
+    dcat = ctx.upload(cat)
+    D = 0.6
+    outs = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in KINDS}
+    assert _call(ctx, fn, dcat, g, outs, D) == 0
+    ctx.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        assert _call(ctx, fn, dcat, g, outs, D) == 0
+    ctx.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    mu = outs["mu"].cpu().numpy()
+    assert np.count_nonzero(np.abs(mu) > 100) > 100
+
+
+def test_noalloc_kmap(env):
+    """The Kmap form (per-halo D_LS/D_OS weights, two source planes) against
+    lt_hessian_maps with kmap, on two calls in a row."""
+    import torch
+    ctx, fn = env
+    cat = catalog.cluster_galaxy_catalog(2, 300, 11)
+    cat.dlsds = np.where(np.arange(cat.n) < 150, 0.55, 0.75)
+    g = catalog.Grid.square(100., 768)
+    dcat = ctx.upload(cat)
+    kinds = ("hess_a", "hess_b", "mass", "mu")
+    ref = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in kinds}
+    ctx.hessian_maps(dcat, g, list(kinds), precision="fp32c", kmap=True, dlsds=1.0, mult=1.3,
+                     out=list(ref.values()))
+    ctx.synchronize()
+    ref = {k: v.cpu().numpy() for k, v in ref.items()}
+    for call in range(2):
+        outs = {k: torch.full((g.ny, g.nx), np.nan, dtype=torch.float64, device="cuda") for k in kinds}
+        st = _call(ctx, fn, dcat, g, outs, 1.0, kmap=1, mult=1.3)
+        assert st == 0, (call, lt.STATUS.get(st), ctx._lib.lt_last_error(ctx.handle))
+        ctx.synchronize()
+        for k, v in outs.items():
+            got = v.cpu().numpy()
+            assert max_rel_err(got, ref[k]) <= TOL, (call, k)
+
+
 def test_noalloc_rejects_what_it_cannot_serve(env):
     import torch
     ctx, fn = env
