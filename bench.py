@@ -56,9 +56,9 @@ FLOPS_PER_PAIR = 182 + 760
 # says whether the timed build is that one.
 KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
                   "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
-INST_SOURCES_SHA = "pending"
-INST_PER_PAIR_FP32C_LENS = 278.7
-FP32_FLOPS_PER_PAIR_FP32C_LENS = 241.1
+INST_SOURCES_SHA = "5a5cca52e2a71d90"
+INST_PER_PAIR_FP32C_LENS = 193.8
+FP32_FLOPS_PER_PAIR_FP32C_LENS = 138.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
 TRAFFIC_FP32C_LENS_4096 = 19494912 + 631581696

@@ -33,7 +33,13 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
         for (int k = 0; k < P; k++) {
             if ((OP & OP_GRAD) && (OP & OP_GFX)) grad_pair_fast<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
             if ((OP & OP_GRAD) && !(OP & OP_GFX)) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
-            if (OP & OP_HESS) {
+            if ((OP & OP_HESS) && (OP & OP_NI)) {
+                const Hess64 t = hess_term<TYPE>(r, px[k], py, w);
+                acc.hxx[k] = __dadd_rn(acc.hxx[k], t.xx);
+                acc.hyy[k] = __dadd_rn(acc.hyy[k], t.yy);
+                acc.hxy[k] = __dadd_rn(acc.hxy[k], t.xy);
+            }
+            if ((OP & OP_HESS) && !(OP & OP_NI)) {
                 Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
                 hess_pair<TYPE>(r, px[k], py, w, hh);
                 acc.hxx[k] = hh.xx;
@@ -194,13 +200,13 @@ __device__ __forceinline__ void eval64_chunk(const lt_rec64 *recs, int count, co
         const double w = kmap ? r.w : 1.0;
 #pragma unroll
         for (int k = 0; k < P; k++) {
-            if (OP & OP_HESS) {
-                Hess64 hh = {0., 0., 0.};
-                hess_pair<TYPE>(r, px[k], py, w, hh);
-                add_hess64(acc, k, hh);
+            if (OP & OP_HESS) add_hess64(acc, k, hess_term<TYPE>(r, px[k], py, w));
+            if (OP & OP_POT) acc.psi[k] = __dadd_rn(acc.psi[k], pot_term<TYPE>(r, px[k], py));
+            if (OP & OP_GRAD) {
+                const double2 t = grad_term<TYPE>(r, px[k], py);
+                acc.gx[k] = __dadd_rn(acc.gx[k], t.x);
+                acc.gy[k] = __dadd_rn(acc.gy[k], t.y);
             }
-            if (OP & OP_POT) pot_pair_fast<TYPE>(r, px[k], py, acc.psi[k]);
-            if (OP & OP_GRAD) grad_pair_fast<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
         }
     }
 }
@@ -243,13 +249,13 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
                 const double w = kmap ? r64.w : 1.0;
 #pragma unroll
                 for (int k = 0; k < P; k++) {
-                    if (OP & OP_HESS) {
-                        Hess64 hh = {0., 0., 0.};
-                        hess_pair<TYPE>(r64, px[k], py, w, hh);
-                        add_hess64(acc, k, hh);
+                    if (OP & OP_HESS) add_hess64(acc, k, hess_term<TYPE>(r64, px[k], py, w));
+                    if (OP & OP_GRAD) {
+                        const double2 t = grad_term<TYPE>(r64, px[k], py);
+                        acc.gx[k] = __dadd_rn(acc.gx[k], t.x);
+                        acc.gy[k] = __dadd_rn(acc.gy[k], t.y);
                     }
-                    if (OP & OP_GRAD) grad_pair_fast<TYPE>(r64, px[k], py, acc.gx[k], acc.gy[k]);
-                    if (OP & OP_POT) pot_pair_fast<TYPE>(r64, px[k], py, acc.psi[k]);
+                    if (OP & OP_POT) acc.psi[k] = __dadd_rn(acc.psi[k], pot_term<TYPE>(r64, px[k], py));
                 }
             } else {
 #pragma unroll
@@ -292,8 +298,8 @@ __device__ __forceinline__ void eval32_chunk(const lt_rec32 *recs, const lt_rec6
  * of independent errors, kEpsTerm32 kSpread32 times the root sum of squares of the terms,
  * which also covers a pixel dominated by one term at its worst error; the convergence
  * adds kEpsBlock32 of the (one-signed) sum of its terms for the coherent part of the
- * blocks' rounding:
- *   |d det| <= 2 D (|1 - kappa D| dk + (|gamma1 D| + |gamma2 D|) dg). */
+ * blocks' rounding.  The two shear components' errors being independent too,
+ *   |d det| <= 2 D (|1 - kappa D| dk + |gamma D| dg). */
 constexpr float kEpsTerm32 = 2.0e-7f;
 constexpr float kSpread32 = 5.f;
 constexpr float kEpsBlock32 = 1.2e-7f;
@@ -312,7 +318,8 @@ __device__ __forceinline__ void fp32c_total(const Acc32<P> &acc, int k, double D
     det = sub(sub(mul(omk, omk), mul(g1d, g1d)), mul(g2d, g2d));
     const float dk = __fmaf_rn(kEpsTerm32 * kSpread32, __fsqrt_rn(acc.mk[k]), __fmul_rn(kEpsBlock32, acc.ml[k]));
     const float dg = __fmul_rn(kEpsTerm32 * kSpread32, __fsqrt_rn(acc.mg[k]));
-    det_err = mul(mul(2., D), add(mul(fabs(omk), (double)dk), mul(add(fabs(g1d), fabs(g2d)), (double)dg)));
+    const double gd = sqr(add(mul(g1d, g1d), mul(g2d, g2d)));
+    det_err = mul(mul(2., D), add(mul(fabs(omk), (double)dk), mul(gd, (double)dg)));
 }
 
 /* Pixel total of the FP32C deflection sums. */
@@ -323,11 +330,15 @@ __device__ __forceinline__ void fp32c_grad_total(const Acc32<P> &acc, int k, dou
     gy = acc.gy[k];
 }
 
-/* True when the FP32 part's error bound on the magnification |mu| |d det| / |det| exceeds
- * mu_tol (a pixel near a critical curve): the pixel is then recomputed in FP64. */
+/* True when the FP32 part's error bound on the magnification exceeds mu_tol of
+ * max(|mu|, 1) (near a critical curve the determinant amplifies the error of the sums):
+ * |d mu| = mu^2 |d det| <= mu_tol max(|mu|, 1), i.e. |d det| <= mu_tol |det| max(1, |det|).
+ * (A map of mu is judged against max(|mu|, its RMS), and its RMS is at least about 1, the
+ * magnification far from any lens.)  The pixel is then recomputed in FP64. */
 __device__ __forceinline__ bool fp32c_flag(double det, double det_err, double mu_tol)
 {
-    return !(det_err <= mu_tol * fabs(det));
+    const double ad = fabs(det);
+    return !(det_err <= mu_tol * ad * fmax(1., ad));
 }
 
 } // namespace lt

@@ -181,9 +181,9 @@ static int launch_shape(int shape, const GridArgs &a, int num_sms, cudaStream_t 
 int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool list_mode, int shape)
 {
     cudaStream_t s = (cudaStream_t)stream;
-    if (list_mode) {
+    if (list_mode) { /* the FP32C recomputation pass: the out-of-line fast Hessian */
         if (op != OP_HESS) return (int)cudaErrorInvalidValue;
-        return launch_op<OP_HESS, 1, true, 2>(args, num_sms, s);
+        return launch_op<OP_HESS | OP_NI, 1, true, 2>(args, num_sms, s);
     }
     switch (op) {
     case OP_GRAD: return launch_shape<OP_GRAD>(shape, args, num_sms, s);

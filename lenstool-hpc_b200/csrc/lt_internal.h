@@ -52,10 +52,10 @@ struct lt_rec32;
 
 namespace lt {
 
-/* FP32C: a pixel whose bound on the FP32 part's relative error of mu, |d det| / |det|,
+/* FP32C: a pixel whose bound on the FP32 part's error of mu, relative to max(|mu|, 1),
  * exceeds this is recomputed in FP64 (near a critical curve the determinant amplifies
- * the error of the sums as |mu|) */
-constexpr double kMuTol32 = 4.0e-7;
+ * the error of the sums as |mu|); the maps are held to 1e-6 */
+constexpr double kMuTol32 = 5.0e-7;
 
 /* FP32C catalogue (lt_catalog::aux_desc): FP32 records + a chunk list over both record
  * kinds (chunk.pad & CHUNK_FP32: FP32 records of recs32, else FP64 records of recs64). */

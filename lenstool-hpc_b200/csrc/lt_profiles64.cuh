@@ -541,4 +541,34 @@ __device__ __forceinline__ void hess_pair(const lt_rec64 &h, double px, double p
     rotate_acc(m, h.cs, h.sn, acc);
 }
 } // namespace ex
+
+/* The FP64 terms of one pair as out-of-line functions, for the FP32C path's FP64 work (its
+ * cluster-scale halos, the near field of its galaxies, the recomputation near critical
+ * curves).  Compiled once per profile type, they round alike in every kernel that calls
+ * them, whatever else that kernel computes, so a map is the same from the grid kernels
+ * and the work-queue tiles bit for bit; and their registers are not the calling pair
+ * loop's. */
+template <int TYPE>
+__device__ __noinline__ Hess64 hess_term(const lt_rec64 &h, double px, double py, double w)
+{
+    Hess64 a = {0., 0., 0.};
+    hess_pair<TYPE>(h, px, py, w, a);
+    return a;
+}
+
+template <int TYPE>
+__device__ __noinline__ double pot_term(const lt_rec64 &h, double px, double py)
+{
+    double p = 0.;
+    pot_pair_fast<TYPE>(h, px, py, p);
+    return p;
+}
+
+template <int TYPE>
+__device__ __noinline__ double2 grad_term(const lt_rec64 &h, double px, double py)
+{
+    double gx = 0., gy = 0.;
+    grad_pair_fast<TYPE>(h, px, py, gx, gy);
+    return make_double2(gx, gy);
+}
 } // namespace lt

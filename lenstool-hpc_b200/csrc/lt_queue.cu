@@ -294,16 +294,16 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
         const int qx = tile_x0 + l % (32 * P), qy = tile_y0 + l / (32 * P);
         double qpx[1] = {pixel_x(a, have ? qx : 0)};
         const double qpy = pixel_y(a, have ? qy : 0);
-        Acc64<OP_HESS, 1> h;
+        Acc64<OP_HESS | OP_NI, 1> h;
         h.hxx[0] = h.hyy[0] = h.hxy[0] = 0.;
         ok = walk_chunks(st, a.chunks, a.nchunks, a.recs, nullptr, status,
                          [&](const lt_chunk &c, const unsigned char *buf) {
                              if (!have) return;
                              const lt_rec64 *recs = reinterpret_cast<const lt_rec64 *>(buf);
                              switch (c.type) {
-                             case 81: eval_chunk64<OP_HESS, 1, 81>(recs, c.count, qpx, qpy, a.kmap, h); break;
-                             case 8: eval_chunk64<OP_HESS, 1, 8>(recs, c.count, qpx, qpy, a.kmap, h); break;
-                             case 5: eval_chunk64<OP_HESS, 1, 5>(recs, c.count, qpx, qpy, a.kmap, h); break;
+                             case 81: eval_chunk64<OP_HESS | OP_NI, 1, 81>(recs, c.count, qpx, qpy, a.kmap, h); break;
+                             case 8: eval_chunk64<OP_HESS | OP_NI, 1, 8>(recs, c.count, qpx, qpy, a.kmap, h); break;
+                             case 5: eval_chunk64<OP_HESS | OP_NI, 1, 5>(recs, c.count, qpx, qpy, a.kmap, h); break;
                              default: break;
                              }
                          });

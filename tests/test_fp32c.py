@@ -162,3 +162,53 @@ def test_fp32c_deflection(ctx, workload):
     print(f"fp32c deflection max rel err {workload}: {errs}")
     for i in range(2):
         assert errs[i] <= TOL32, (workload, i)
+
+
+def test_fp32c_per_term_errors_of_lone_galaxies(ctx):
+    """The FP32 closed forms term by term: lone galaxy-scale cut dPIEs at random mass
+    ellipticity (0.01-0.6), core (0.01-0.8") and cut (5-50") radii, each alone on a near
+    field (4 rcut) and a far field (150"); outside the halo's FP64 disc every pixel is one
+    FP32 term.  Relative errors against LT_FP64: convergence and the potential against
+    their own values, the shear components against |gamma1| + |gamma2|, the deflection
+    against |alpha|."""
+    import torch
+    rng = np.random.default_rng(7)
+    worst = {"kappa": 0., "gamma": 0., "alpha": 0., "psi": 0.}
+    n = 0
+    while n < 16:
+        sig = float(np.exp(rng.uniform(np.log(80), np.log(300))))
+        em, th = float(rng.uniform(0.01, 0.6)), float(rng.uniform(0, np.pi))
+        rc = float(np.exp(rng.uniform(np.log(0.01), np.log(0.8))))
+        rcut = float(rng.uniform(5, 50))
+        x0, y0 = float(rng.uniform(-1, 1)), float(rng.uniform(-1, 1))
+        cat = catalog.make_catalog([81], [x0], [y0], [sig], [em], [th], [rc], [rcut])
+        b0, e = float(cat.b0[0]), float(cat.ellipticity_potential[0])
+        if b0 >= 5 or e < 1e-3:
+            continue
+        n += 1
+        for half in (4 * rcut, 150.):
+            g = catalog.Grid.square(half, 385)
+            res = {}
+            for prec in ("fp32c", "fp64"):
+                o = [torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for _ in range(6)]
+                ctx.hessian_maps(cat, g, ["hess_a", "hess_b", "hess_c"], precision=prec, out=o[:3])
+                ctx.gradient_grid(cat, g, precision=prec, out=(o[3], o[4]))
+                ctx.potential_grid(cat, g, precision=prec, out=o[5])
+                ctx.synchronize()
+                res[prec] = [x.cpu().numpy() for x in o]
+            a, b, c, ax, ay, ps = res["fp64"]
+            a2, b2, c2, ax2, ay2, ps2 = res["fp32c"]
+            px, py = g.coords()
+            r2 = (px.reshape(g.ny, g.nx) - x0) ** 2 + (py.reshape(g.ny, g.nx) - y0) ** 2
+            m = r2 >= max(b0 / 0.2, 3 * rc) ** 2 * 1.001  # outside the FP64 disc
+            k, k2 = (a + c) / 2, (a2 + c2) / 2
+            g1, g12, g2, g22 = (a - c) / 2, (a2 - c2) / 2, b, b2
+            errs = {"kappa": np.abs(k2 - k) / np.abs(k),
+                    "gamma": np.maximum(np.abs(g12 - g1), np.abs(g22 - g2)) / (np.abs(g1) + np.abs(g2)),
+                    "alpha": np.hypot(ax2 - ax, ay2 - ay) / np.hypot(ax, ay),
+                    "psi": np.abs(ps2 - ps) / np.abs(ps)}
+            for key, err in errs.items():
+                worst[key] = max(worst[key], float(err[m].max()))
+    print("fp32c per-term relative errors, lone dPIEs:", worst)
+    assert worst["kappa"] <= 1.2e-6 and worst["gamma"] <= 1.2e-6
+    assert worst["alpha"] <= 2e-6 and worst["psi"] <= 1.5e-6
