@@ -117,6 +117,7 @@ lt_status make_queue_item(lt_context *ctx, const lt_request *r, int precision, d
         it->recs32 = fc.recs32;
         it->chunks32 = fc.chunks;
         it->nchunks32 = cat->nhalos ? fc.nchunks : 0;
+        it->nie64 = fc.nie;
         it->mu_tol = det ? kMuTol32 : 0.0;
     }
     if (cat->nhalos == 0) a.nchunks = 0;

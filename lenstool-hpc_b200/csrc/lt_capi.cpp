@@ -271,6 +271,11 @@ lt_status lt_create(int device, size_t budget, lt_context **out)
     ctx->shape[LT_FP32C][OP_HESS | OP_POT] = LT_SHAPE4(2, 2, 256, 128);
     ctx->shape[LT_FP32C][OP_GRAD] = LT_SHAPE4(2, 2, 256, 128);
     cudaSetDevice(device);
+    if (configure_kernels32() != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return LT_ERR_CUDA;
+    }
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     ctx->budget = budget ? budget : (size_t)(0.9 * (double)free_b);

@@ -28,13 +28,15 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
 #pragma unroll 1
     for (int h = 0; h < count; h++) {
         const lt_rec64 &r = recs[h];
-        double w = kmap ? r.w : 1.0;
+        /* OP_NI: the staged records are the closed-form records lt_nie64 */
+        const lt_nie64 &rn = reinterpret_cast<const lt_nie64 &>(r);
+        const double w = kmap ? ((OP & OP_NI) ? rn.w : r.w) : 1.0;
 #pragma unroll
         for (int k = 0; k < P; k++) {
             if ((OP & OP_GRAD) && (OP & OP_GFX)) grad_pair_fast<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
             if ((OP & OP_GRAD) && !(OP & OP_GFX)) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
             if ((OP & OP_HESS) && (OP & OP_NI)) {
-                const Hess64 t = hess_term<TYPE>(r, px[k], py, w);
+                const Hess64 t = nie_hess64<TYPE>(rn, px[k], py, w);
                 acc.hxx[k] = __dadd_rn(acc.hxx[k], t.xx);
                 acc.hyy[k] = __dadd_rn(acc.hyy[k], t.yy);
                 acc.hxy[k] = __dadd_rn(acc.hxy[k], t.xy);

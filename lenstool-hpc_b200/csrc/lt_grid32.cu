@@ -89,13 +89,17 @@ lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
     h.nchunks = (int32_t)l64.size();
     h.nchunks_s = (int32_t)l32.size();
     h.nchunks_l = (int32_t)l128.size();
+    std::vector<lt_nie64> nie((size_t)n);
+    for (int i = 0; i < n; i++) pk::pack_nie64(cat->host_recs[i], types[i], nie[i]);
     size_t rb = sizeof(lt_rec32) * r32.size(), cb = sizeof(lt_chunk) * host_chunks.size();
-    const size_t ib = sizeof(int32_t) * (size_t)n;
-    size_t total = sizeof(Fp32cCatalog) + rb + cb + 2 * ib + 64;
+    const size_t ib = sizeof(int32_t) * (size_t)n, nb = sizeof(lt_nie64) * (size_t)n;
+    size_t total = sizeof(Fp32cCatalog) + nb + rb + cb + 2 * ib + 64;
     void *mem = nullptr;
     lt_status st = dev_alloc(ctx, &mem, total);
     if (st != LT_OK) return st;
     char *base = (char *)mem;
+    h.nie = (lt_nie64 *)(base + 64);
+    base += nb;
     h.recs32 = (lt_rec32 *)(base + 64);
     h.chunks = (lt_chunk *)(base + 64 + rb);
     h.chunks_s = h.chunks + l64.size();
@@ -107,6 +111,7 @@ lt_status prepare_catalog_extensions(lt_context *ctx, lt_catalog *cat)
     if (e == cudaSuccess && cb) e = cudaMemcpy(h.chunks, host_chunks.data(), cb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && ib) e = cudaMemcpy(h.idx32, idx32.data(), ib, cudaMemcpyHostToDevice);
     if (e == cudaSuccess && ib) e = cudaMemcpy(h.types, types.data(), ib, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && nb) e = cudaMemcpy(h.nie, nie.data(), nb, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         dev_free(ctx, mem, total);
         return cuda_fail(ctx, e, "FP32 catalogue upload");
@@ -306,6 +311,21 @@ const int kShapes32[] = {LT_SHAPE(1, 1), LT_SHAPE(1, 2), LT_SHAPE(2, 1), LT_SHAP
                          LT_SHAPE4(2, 3, 128, 64), LT_SHAPE4(2, 4, 128, 64)};
 const int kNumShapes32 = (int)(sizeof(kShapes32) / sizeof(kShapes32[0]));
 
+/* Allow every FP32C kernel the dynamic shared memory of the largest stage (two 128-record
+ * stages, 64 KB) on the current device: once per context, not per launch (the attribute
+ * call is far slower than a small launch). */
+int configure_kernels32()
+{
+    const size_t smem = 2 * (size_t)128 * sizeof(lt_rec64);
+    for (int op : {(int)OP_HESS, (int)OP_POT, (int)(OP_HESS | OP_POT), (int)OP_GRAD})
+        for (int k = 0; k < kNumShapes32; k++) {
+            const cudaError_t e = cudaFuncSetAttribute(pick_kernel32(op, kShapes32[k]),
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return (int)e;
+        }
+    return (int)cudaSuccess;
+}
+
 bool shape32_ok(int shape)
 {
     const int cap = shape_cap(shape);
@@ -339,11 +359,7 @@ static int launch_pass1(lt_context *ctx, const Fp32cCatalog &fc, int op, C32Args
     A.recs32 = fc.recs32;
     A.g.tiles_x = (A.g.nx + 32 * P - 1) / (32 * P);
     A.g.ntiles = A.g.tiles_x * ((A.g.ny + NT / 32 - 1) / (NT / 32));
-    const size_t smem = 2 * (size_t)cap * sizeof(lt_rec64);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return (int)e;
-    }
+    const size_t smem = 2 * (size_t)cap * sizeof(lt_rec64); /* allowed once by configure_kernels32 */
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem);
     if (per_sm < 1) per_sm = 1;
@@ -401,6 +417,7 @@ int launch_fp32c(lt_context *ctx, const lt_catalog *cat, int op, GridArgs &a, vo
     r.list = A.list;
     r.list_count = A.list_count;
     r.list_cap = A.list_cap;
+    r.recs = reinterpret_cast<const lt_rec64 *>(fc.nie); /* the closed-form FP64 records */
     err = launch_grid64_list(OP_HESS, r, ctx->num_sms, stream);
     count_launch(1);
     pass_mark(ctx, s, 2);
@@ -435,6 +452,7 @@ int launch_fp32c_with_list(lt_context *ctx, const lt_catalog *cat, GridArgs &a, 
     r.list = A.list;
     r.list_count = A.list_count;
     r.list_cap = A.list_cap;
+    r.recs = reinterpret_cast<const lt_rec64 *>(fc.nie); /* the closed-form FP64 records */
     err = launch_grid64_list(OP_HESS, r, ctx->num_sms, stream);
     count_launch(1);
     return err;

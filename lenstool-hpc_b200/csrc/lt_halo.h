@@ -45,6 +45,22 @@ struct alignas(16) lt_rec64 {
 };
 static_assert(sizeof(lt_rec64) == 256, "record size");
 
+/* The FP64 record of the closed-form Hessian (the real-valued forms of
+ * lt_profiles32.cuh in FP64: q = (1-e)/(1+e), s = (1+e) r, K = b0 (1-e) t05 / 2), used by
+ * the FP32C path's FP64 recomputation.  Same size as lt_rec64 so that the FP64 chunk
+ * lists and staging serve both.  A type-5 (SIS) record uses q2 = 1 - e, k = 1 + e,
+ * K = b0 (1-e)(1+e). */
+struct alignas(16) lt_nie64 {
+    double x0, y0, cs, sn;
+    double c2t, s2t, w, k;
+    double q2, sc, st, ds;
+    double q2sc2, q2st2, dq2s2, opsc2;
+    double opst2, opds2, tsc, tst;
+    double K, Kc1sc2, Kc1st2, pad0;
+    double pad[8];
+};
+static_assert(sizeof(lt_nie64) == sizeof(lt_rec64), "record size");
+
 /* A chunk: a run of consecutive halos of one type, at most LT_CHUNK halos long.  The
  * grid kernels walk the chunk list; runs of equal type are the reference's dispatch unit
  * (src/gradient.cpp:899-929). */

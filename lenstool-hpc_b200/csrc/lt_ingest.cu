@@ -36,6 +36,7 @@ __device__ __forceinline__ void flag(int32_t *status, int32_t code) { atomicCAS(
 struct CatRecs {
     lt_rec64 *recs;
     lt_rec32 *recs32;
+    lt_nie64 *nie;
     const int32_t *idx32;
 };
 
@@ -48,6 +49,9 @@ __device__ __forceinline__ bool store_records(const CatRecs &c, int i, int t, do
     lt_rec64 r;
     pk::pack64(t, x, y, cs, sn, b0, eps, rc, rcut, c.recs[i].w, r);
     c.recs[i] = r;
+    lt_nie64 q;
+    pk::pack_nie64(r, t, q);
+    c.nie[i] = q;
     const int j = c.idx32[i];
     if (j >= 0) {
         lt_rec32 o;
@@ -208,6 +212,7 @@ static CatRecs recs_of(const lt_catalog *cat)
     CatRecs c;
     c.recs = cat->recs;
     c.recs32 = fc.recs32;
+    c.nie = fc.nie;
     c.idx32 = fc.idx32;
     return c;
 }

@@ -44,7 +44,7 @@ struct lt_catalog {
     size_t aux_bytes = 0;
     void *stage = nullptr;               /* device staging of host parameters (lt_catalog_update) */
     size_t stage_bytes = 0;
-    alignas(16) unsigned char aux_desc[64]; /* FP32C descriptor (host) */
+    alignas(16) unsigned char aux_desc[96]; /* FP32C descriptor (host) */
 };
 
 struct lt_rec32;
@@ -68,6 +68,7 @@ struct Fp32cCatalog {
     int32_t n32;
     int32_t *idx32;  /* per halo: its FP32 record, or -1 for an FP64-class halo (device) */
     int32_t *types;  /* per halo profile type (device) */
+    lt_nie64 *nie;   /* per halo (upload order): the FP64 closed-form record of the recomputation */
 };
 
 void count_launch(uint64_t n);
@@ -81,6 +82,8 @@ void noalloc_forget(int device);
 extern const int kShapes32[];
 extern const int kNumShapes32;
 bool shape32_ok(int shape);
+/* allow the FP32C kernels their largest shared-memory stage on the current device */
+int configure_kernels32();
 void set_error(lt_context *ctx, const char *fmt, ...);
 lt_status cuda_fail(lt_context *ctx, cudaError_t e, const char *what);
 lt_status dev_alloc(lt_context *ctx, void **p, size_t bytes);

@@ -221,5 +221,48 @@ LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     if (core_r2 > mul(near_r, near_r)) o.rnear2 = f32(core_r2);
 }
 
+/* The FP64 closed-form record (lt_halo.h: lt_nie64) of any halo. */
+LT_HD inline void pack_nie64(const lt_rec64 &r, int type, lt_nie64 &o)
+{
+    memset(&o, 0, sizeof(o));
+    o.x0 = r.x0;
+    o.y0 = r.y0;
+    o.cs = r.cs;
+    o.sn = r.sn;
+    o.c2t = sub(mul(r.cs, r.cs), mul(r.sn, r.sn));
+    o.s2t = mul(mul(2., r.cs), r.sn);
+    o.w = r.w;
+    const double e = r.eps;
+    if (type == 5) {
+        o.q2 = sub(1., e);
+        o.k = add(1., e);
+        o.K = mul(mul(r.b0, sub(1., e)), add(1., e));
+        return;
+    }
+    const double ope = add(1., e), ome = sub(1., e);
+    const double q = div(ome, ope), q2 = mul(q, q), opq2 = add(1., q2);
+    const double t05 = (type == 81) ? div(r.rcut, sub(r.rcut, r.rc)) : 1.0;
+    const double K = mul(0.5, mul(mul(r.b0, ome), t05));
+    const double sc = mul(ope, r.rc), st = mul(ope, r.rcut);
+    const double sc2 = mul(sc, sc), st2 = mul(st, st), ds2 = mul(sub(sc, st), add(sc, st));
+    const double c1 = sub(q2, 1.);
+    o.q2 = q2;
+    o.k = div(mul(2., sqr(e)), ope);
+    o.sc = sc;
+    o.st = st;
+    o.ds = sub(sc, st);
+    o.q2sc2 = mul(q2, sc2);
+    o.q2st2 = mul(q2, st2);
+    o.dq2s2 = mul(q2, ds2);
+    o.opsc2 = mul(opq2, sc2);
+    o.opst2 = mul(opq2, st2);
+    o.opds2 = mul(opq2, ds2);
+    o.tsc = mul(2., sc);
+    o.tst = mul(2., st);
+    o.K = K;
+    o.Kc1sc2 = mul(mul(K, c1), sc2);
+    o.Kc1st2 = mul(mul(K, c1), st2);
+}
+
 } // namespace pk
 } // namespace lt

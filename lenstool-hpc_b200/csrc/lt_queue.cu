@@ -296,7 +296,7 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
         const double qpy = pixel_y(a, have ? qy : 0);
         Acc64<OP_HESS | OP_NI, 1> h;
         h.hxx[0] = h.hyy[0] = h.hxy[0] = 0.;
-        ok = walk_chunks(st, a.chunks, a.nchunks, a.recs, nullptr, status,
+        ok = walk_chunks(st, a.chunks, a.nchunks, reinterpret_cast<const lt_rec64 *>(it.nie64), nullptr, status,
                          [&](const lt_chunk &c, const unsigned char *buf) {
                              if (!have) return;
                              const lt_rec64 *recs = reinterpret_cast<const lt_rec64 *>(buf);

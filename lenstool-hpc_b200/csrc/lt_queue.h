@@ -33,7 +33,7 @@ struct alignas(16) QItem {
     double mu_tol;              /* FP32C: recompute pixels whose FP32 error bound on mu exceeds
                                    this in FP64 (0: none) */
     uint32_t *host_flag;        /* mapped host word set to seq + 1 on completion, or null */
-    int64_t pad1;
+    const lt_nie64 *nie64;      /* FP32C: the closed-form FP64 records of the recomputation */
 };
 static_assert(sizeof(QItem) % 16 == 0, "QItem is copied in 16-byte units");
 

@@ -67,6 +67,9 @@ def test_fp32c_workload_maps(ctx):
         assert errs[k]["max"] <= TOL32, (k, errs[k])
     # the excluded pixels are few: the critical curves of a 4096^2 map
     assert errs["mu"]["pixels_mu_gt_cut"] < 1e-2 * g.npix
+    # and their Hessian maps come from the FP64 recomputation (the closed forms in FP64)
+    for k in ("kappa", "gamma1", "gamma2"):
+        assert errs[k]["max_mu_gt_cut"] <= 1e-10, (k, errs[k])
 
 
 @pytest.mark.parametrize("cluster_type", [81, 8, 5])
