@@ -42,6 +42,10 @@ sys.path.insert(0, str(ROOT))
 
 WORKLOAD = "maps_1000h_4096"
 METRIC = "halo x pixel evals/s (Hessian + potential, lens maps kappa/gamma1/gamma2/mu/psi)"
+# the metric of the single-kind runs (--maps), which are profiling cases, not the bench line
+METRIC_OF_MAPS = {"all": METRIC, "hessian": "halo x pixel evals/s (Hessian, maps kappa/gamma1/gamma2/mu)",
+                  "potential": "halo x pixel evals/s (potential)",
+                  "deflection": "halo x pixel evals/s (deflection x/y)"}
 # weighted flop census per pair of the reference's own formulas (fixed convention:
 # +,-,* = 1, fma = 2, div = sqrt = 4, log = atan2 = 20): dPIE Hessian 182
 # (src/gradient2.cpp:92-167, :54-83) + dPIE potential 760 (src/potential_GPU.cu:47-116 with
@@ -56,12 +60,12 @@ FLOPS_PER_PAIR = 182 + 760
 # says whether the timed build is that one.
 KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
                   "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
-INST_SOURCES_SHA = "5a5cca52e2a71d90"
+INST_SOURCES_SHA = "35db7a94bf60f0d6"
 INST_PER_PAIR_FP32C_LENS = 193.8
 FP32_FLOPS_PER_PAIR_FP32C_LENS = 138.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
-TRAFFIC_FP32C_LENS_4096 = 19494912 + 631581696
+TRAFFIC_FP32C_LENS_4096 = 15976192 + 633806848
 
 
 def _package():
@@ -289,6 +293,7 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
            "step": "lt_bayes_apply of the rows (HBM) + one lt_batch graph",
            "shape": dict(batch.config(), autotuned=tune)}
     # the sets as host catalogues (the reference's host-side row update), for the plain loop
+    plain_sample = min(plain_sample, n_sets)
     sets = [bayes.catalog_from_state(model, bayes.reference_state(model, (), cols, rows[i]))
             for i in range(plain_sample)]
     # the reference's bayes-map loop (utils/maps/main.cpp:428-587): one launch per map and
@@ -772,7 +777,8 @@ def main():
                 cpu = {"value": None, "unit": "evals/s", "kind": "reference", "cores": os.cpu_count(),
                        "sample": f"unavailable: {ex}"}
         line = {
-            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+            "metric": METRIC_OF_MAPS[args.maps], "value": value, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps,
             "warmup": warmup, "ms_per_step": 1e3 * elapsed / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.precision == "fp32c" else "f64",
             "data": "synthetic",

@@ -2,6 +2,7 @@
  * lt_capi.cpp -- the extern "C" entry points of include/lt_b200.h: contexts, catalogue
  * validation/packing/upload, and the grid calls (argument checks, host staging, launch).
  */
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
@@ -302,6 +303,7 @@ lt_status lt_destroy(lt_context *ctx)
     dev_free(ctx, ctx->scratch, ctx->scratch_bytes);
     dev_free(ctx, ctx->list, ctx->list_bytes);
     dev_free(ctx, ctx->status, 64);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     destroy_extensions(ctx);
     for (cudaEvent_t e : ctx->ev_marks) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
@@ -430,6 +432,10 @@ lt_status lt_synchronize(lt_context *ctx, void *stream)
 
 /* ------------------------------------------------------------- grid calls ---- */
 
+/* host-output calls: the grid in about this many bands of rows, of at least this many rows */
+static const int kHostBands = 8;
+static const int kMinBandRows = 64;
+
 bool lt::grid_ok(const lt_grid *g)
 {
     return g && g->nx > 0 && g->ny > 0 && std::isfinite(g->xmin) && std::isfinite(g->ymin) &&
@@ -493,36 +499,73 @@ lt_status lt::run_grid(lt_context *ctx, const lt_catalog *cat, const lt_grid *g,
     a.scale = scale;
     a.status = ctx->status;
     cudaStream_t s = (cudaStream_t)stream;
-    int err;
-    if (cat->nhalos == 0) {
-        for (int i = 0; i < nout; i++) cudaMemsetAsync(dev_out[i], 0, plane, s);
-        err = cudaSuccess;
-        if (kinds[0] != KIND_GRAD_X) {
+    /* the kernels of one band of rows (the whole grid for device outputs) */
+    auto launch = [&](GridArgs &b) -> int {
+        if (cat->nhalos == 0) {
+            for (int i = 0; i < nout; i++) cudaMemsetAsync(b.out[i], 0, sizeof(double) * (size_t)b.nx * b.ny, s);
+            if (kinds[0] == KIND_GRAD_X) return (int)cudaSuccess;
             /* maps of an empty catalogue: evaluate the epilogue on zero sums */
-            err = launch_epilogue_zero(a, ctx->num_sms, s);
             count_launch(1);
+            return launch_epilogue_zero(b, ctx->num_sms, s);
         }
-    } else if (precision == LT_FP64) {
-        /* the Hessian with the reference's rounding sequence, the potential through its
-         * pi05 formula */
-        const int xop = ((op & OP_HESS) ? ((op & ~OP_HESS) | OP_HEX) : op) | ((op & OP_POT) ? OP_PEX : 0);
-        err = launch_grid64_tiled(xop, a, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
-    } else if (precision == LT_FP64_FAST) {
-        /* the dPIE deflection as log(1 + eps) (a deflection-only call: no kernel combines it) */
-        const int fop = op == OP_GRAD ? (OP_GRAD | OP_GFX) : op;
-        err = launch_grid64_tiled(fop, a, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][op & 7]);
-    } else {
-        err = launch_fp32c(ctx, cat, op, a, s);
-    }
-    if (err != cudaSuccess) return cuda_fail(ctx, (cudaError_t)err, "grid kernel launch");
-    if (host) {
-        for (int i = 0; i < nout; i++) {
-            cudaError_t e = cudaMemcpyAsync(outs[i], dev_out[i], plane, cudaMemcpyDeviceToHost, s);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "result copy");
+        if (precision == LT_FP64) {
+            /* the Hessian with the reference's rounding sequence, the potential through its
+             * pi05 formula */
+            const int xop = ((op & OP_HESS) ? ((op & ~OP_HESS) | OP_HEX) : op) | ((op & OP_POT) ? OP_PEX : 0);
+            return launch_grid64_tiled(xop, b, ctx->num_sms, s, ctx->shape[LT_FP64][op & 7]);
         }
-        return lt_synchronize(ctx, stream);
+        if (precision == LT_FP64_FAST) {
+            /* the dPIE deflection as log(1 + eps) (a deflection-only call: no kernel combines it) */
+            const int fop = op == OP_GRAD ? (OP_GRAD | OP_GFX) : op;
+            return launch_grid64_tiled(fop, b, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][op & 7]);
+        }
+        return launch_fp32c(ctx, cat, op, b, s);
+    };
+    if (!host) {
+        const int err = launch(a);
+        if (err != cudaSuccess) return cuda_fail(ctx, (cudaError_t)err, "grid kernel launch");
+        return LT_OK;
     }
-    return LT_OK;
+    /* Host outputs: the grid in bands of rows, each band's planes copied to the host on a
+     * second stream while the next bands compute.  Every band is launched before the first
+     * copy is issued, since a copy into pageable memory returns only once it is done.
+     * Bands start on multiples of 8 rows, the kernels' tile height, so every warp covers
+     * the pixels it covers in one launch over the whole grid and the maps are the same
+     * bit for bit. */
+    int band = (int)(((long)g->ny + kHostBands - 1) / kHostBands);
+    band = (band + 7) / 8 * 8;
+    if (band < kMinBandRows) band = kMinBandRows;
+    if (!ctx->copy_stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "copy stream");
+    }
+    std::vector<cudaEvent_t> done;
+    int err = cudaSuccess;
+    for (int j0 = 0; j0 < g->ny; j0 += band) {
+        GridArgs b = a;
+        b.ny = std::min(band, g->ny - j0);
+        b.jstart = g->jstart + j0;
+        for (int i = 0; i < nout; i++) b.out[i] = dev_out[i] + (size_t)j0 * g->nx;
+        err = launch(b);
+        cudaEvent_t ev;
+        if (err == cudaSuccess) err = (int)cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (err != cudaSuccess) break;
+        done.push_back(ev);
+        cudaEventRecord(ev, s);
+    }
+    for (size_t k = 0; k < done.size() && err == cudaSuccess; k++) {
+        const int j0 = (int)k * band;
+        const size_t off = (size_t)j0 * g->nx, n = (size_t)std::min(band, g->ny - j0) * g->nx;
+        cudaStreamWaitEvent(ctx->copy_stream, done[k], 0);
+        for (int i = 0; i < nout && err == cudaSuccess; i++)
+            err = (int)cudaMemcpyAsync(outs[i] + off, dev_out[i] + off, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                       ctx->copy_stream);
+    }
+    const cudaError_t se = cudaStreamSynchronize(ctx->copy_stream);
+    for (cudaEvent_t ev : done) cudaEventDestroy(ev);
+    if (err != cudaSuccess) return cuda_fail(ctx, (cudaError_t)err, "grid kernel launch or result copy");
+    if (se != cudaSuccess) return cuda_fail(ctx, se, "result copy");
+    return lt_synchronize(ctx, stream);
 }
 
 /* Tile bookkeeping shared by the launchers. */

@@ -25,6 +25,7 @@ struct lt_context {
     void *list = nullptr;      /* pixel list of the FP32C recomputation pass (+ count) */
     size_t list_bytes = 0;
     int shape[3][8] = {};      /* kernel shape per [precision][sums mask], LT_SHAPE4() */
+    cudaStream_t copy_stream = nullptr; /* host-output calls: band copies overlap the next band */
     /* pass timing (lt_set_pass_timing): CUDA events around the passes of FP32C calls */
     bool timing = false;
     std::vector<cudaEvent_t> ev_pool;   /* created events, reused */

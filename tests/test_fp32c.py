@@ -215,3 +215,19 @@ def test_fp32c_per_term_errors_of_lone_galaxies(ctx):
     print("fp32c per-term relative errors, lone dPIEs:", worst)
     assert worst["kappa"] <= 1.2e-6 and worst["gamma"] <= 1.2e-6
     assert worst["alpha"] <= 2e-6 and worst["psi"] <= 1.5e-6
+
+
+@pytest.mark.parametrize("precision", ["fp32c", "fp64", "fp64fast"])
+def test_host_outputs_in_bands_equal_device_outputs(ctx, precision):
+    """Host-output calls run the grid in bands of rows (the copy of one band overlaps the next
+    band's kernels); the bands start on the kernels' tile rows, so the maps equal a
+    device-output call over the whole grid bit for bit."""
+    import torch
+    cat = catalog.cluster_galaxy_catalog(2, 120, 31)
+    g = catalog.Grid(-90., 90., -60., 70., 600, 523)
+    host = ctx.lens_maps(cat, g, precision=precision, dlsds=0.63)
+    dev = {k: torch.empty((g.ny, g.nx), dtype=torch.float64, device="cuda") for k in host}
+    ctx.lens_maps(cat, g, precision=precision, dlsds=0.63, out=dev)
+    ctx.synchronize()
+    for k in host:
+        assert np.array_equal(host[k], dev[k].cpu().numpy()), (precision, k)
