@@ -60,12 +60,12 @@ FLOPS_PER_PAIR = 182 + 760
 # says whether the timed build is that one.
 KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
                   "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
-INST_SOURCES_SHA = "35db7a94bf60f0d6"
-INST_PER_PAIR_FP32C_LENS = 193.8
-FP32_FLOPS_PER_PAIR_FP32C_LENS = 138.4
+INST_SOURCES_SHA = "e10d46a7870db5c2"
+INST_PER_PAIR_FP32C_LENS = 156.1
+FP32_FLOPS_PER_PAIR_FP32C_LENS = 130.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
-TRAFFIC_FP32C_LENS_4096 = 15976192 + 633806848
+TRAFFIC_FP32C_LENS_4096 = 14123264 + 633822976
 
 
 def _package():
@@ -459,21 +459,25 @@ def bench_serving(ctx, precision, n_requests=96, rate=200.0, plain_sample=None, 
     res["at_70pct_capacity"] = dict(run(arrivals * rate / r70), rate_per_s=r70)
     # one plain call per request (host outputs / host chi2, the reference's calling
     # pattern), in FP64 and in the server's own precision: every request by default (a
-    # smaller sample is scaled to all requests by the halo x pixel evaluations of their grids)
+    # smaller sample is scaled to all requests by the halo x pixel evaluations of their grids).
+    # The same-precision loop (a few seconds; its host-memory page faults vary from run to
+    # run) is timed twice and the faster pass kept.
     idx = list(range(plain_sample or n_requests))
     sample_evals = float(sum(reqs[i][1] ** 2 * halos(reqs[i][0], reqs[i][2]) for i in idx))
     for prec in dict.fromkeys(("fp64", precision)):
-        t0 = time.perf_counter()
-        for i in idx:
-            k, n, c = reqs[i]
-            g = catalog.Grid.square(100., n)
-            if k == 0:
-                ctx.gradient_grid(dcats[c], g, precision=prec, scale=D)
-            elif k == 1:
-                ctx.hessian_maps(dcats[c], g, list(kinds_of[1]), precision=prec, dlsds=D)
-            else:
-                ctx.chi2(models[c], frame, n, systems, precision=prec)
-        t = time.perf_counter() - t0
+        t = float("inf")
+        for _ in range(1 if prec == "fp64" else 2):
+            t0 = time.perf_counter()
+            for i in idx:
+                k, n, c = reqs[i]
+                g = catalog.Grid.square(100., n)
+                if k == 0:
+                    ctx.gradient_grid(dcats[c], g, precision=prec, scale=D)
+                elif k == 1:
+                    ctx.hessian_maps(dcats[c], g, list(kinds_of[1]), precision=prec, dlsds=D)
+                else:
+                    ctx.chi2(models[c], frame, n, systems, precision=prec)
+            t = min(t, time.perf_counter() - t0)
         t_all = t * evals / sample_evals
         key = "one_request_per_call_" + ("fp64" if prec == "fp64" else "same_precision")
         res[key] = {"precision": prec, "requests_per_s": len(reqs) / t_all, "maps_per_s": nmaps / t_all,

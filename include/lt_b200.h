@@ -284,8 +284,9 @@ lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision,
  * With timing on, every LT_FP32C grid call records CUDA events on its stream around its
  * two passes (pass 1: the FP32C kernel; pass 2: the FP64 recomputation of the pixels
  * near critical curves).  lt_pass_times waits for the last recorded call, returns the
- * summed durations (ms) and the number of calls since the previous read, and starts a
- * new count.  No counterpart in the reference. */
+ * summed durations (ms) and the number of launches since the previous read (a call with
+ * host outputs runs the grid in bands of rows, one launch each), and starts a new count.
+ * No counterpart in the reference. */
 lt_status lt_set_pass_timing(lt_context *ctx, int32_t on);
 lt_status lt_pass_times(lt_context *ctx, double *pass1_ms, double *pass2_ms, int32_t *calls);
 
@@ -488,6 +489,11 @@ int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *r
  * inputs (0 = LT_OK). */
 int lt_eval_fast_math32(int device, int n, const float *y, const float *x, float *atan2_own, float *atan2_cuda,
                         float *sqrt_own, float *atanh_own);
+
+/* The approximate FP32 reciprocal, reciprocal square root and natural logarithm of the
+ * compensated pair loops (the .ftz instruction forms; the logarithm as ln 2 log2 x) and
+ * CUDA's logf, on n host inputs (0 = LT_OK). */
+int lt_eval_approx32(int device, int n, const float *x, float *rcp, float *rsqrt, float *log_own, float *log_cuda);
 
 const char *lt_status_string(lt_status status);
 /* Last error message recorded by the context (never NULL). */

@@ -138,3 +138,38 @@ extern "C" int lt_eval_fast_math32(int device, int n, const float *y, const floa
     cudaFree(d);
     return e == cudaSuccess ? 0 : 4;
 }
+
+/* ---- the approximate reciprocal, reciprocal square root and logarithm of the pair loops ---- */
+
+namespace {
+__global__ void approx32_kernel(const float *x, float *rcp, float *rsq, float *lg, float *lg_cuda, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        rcp[i] = lt::frcp(x[i]);
+        rsq[i] = lt::frsqrt(x[i]);
+        lg[i] = lt::flog(x[i]);
+        lg_cuda[i] = logf(x[i]);
+    }
+}
+} // namespace
+
+extern "C" int lt_eval_approx32(int device, int n, const float *x, float *rcp, float *rsqrt, float *log_own,
+                                float *log_cuda)
+{
+    if (n < 1 || !x || !rcp || !rsqrt || !log_own || !log_cuda) return 1;
+    if (cudaSetDevice(device) != cudaSuccess) return 4;
+    float *d = nullptr;
+    const size_t b = sizeof(float) * (size_t)n;
+    if (cudaMalloc(&d, 5 * b) != cudaSuccess) return 5;
+    cudaError_t e = cudaMemcpy(d, x, b, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        approx32_kernel<<<256, 256>>>(d, d + n, d + 2 * (size_t)n, d + 3 * (size_t)n, d + 4 * (size_t)n, n);
+        lt::count_launch(1);
+        e = cudaMemcpy(rcp, d + n, b, cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(rsqrt, d + 2 * (size_t)n, b, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(log_own, d + 3 * (size_t)n, b, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(log_cuda, d + 4 * (size_t)n, b, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? 0 : 4;
+}

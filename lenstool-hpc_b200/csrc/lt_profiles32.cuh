@@ -80,7 +80,31 @@ __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b);
 __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 } // namespace f32
 
-__device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+/* Reciprocal, reciprocal square root and log2 by the approximate instructions alone
+ * (rcp/rsqrt/lg2.approx, relative error ~2^-23, log2 absolute ~2^-22).  The .ftz forms
+ * flush subnormal operands to zero, which skips the operand scaling the default forms
+ * wrap around the instruction; every operand here is a normal number (a squared radius,
+ * a denominator, a log argument of 2 or more), where both forms return the same value. */
+__device__ __forceinline__ float frcp(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float frsqrt(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+/* Natural logarithm as ln 2 log2(x) for x >= 2 (where the log2 instruction's absolute error
+ * is a few ulp of the result). */
+__device__ __forceinline__ float flog(float x)
+{
+    float r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return __fmul_rn(r, 0.693147182f);
+}
 
 /* Square root to the approximate instruction's accuracy (relative error ~2^-23), for
  * operands whose rounding the compensated path tolerates; zero and denormals give 0. */
@@ -148,19 +172,19 @@ __device__ __forceinline__ float fatanh_third(float s)
 }
 
 /* atanh y for |y| < 1: fatanh_third where |y| <= 1/3, log((1 + y)/(1 - y))/2 above (an
- * argument of 2 or more, where __logf is good to a few ulp). */
+ * argument of 2 or more, where flog is good to a few ulp). */
 __device__ __forceinline__ float fatanh_any(float y)
 {
     using namespace f32;
-    return fabsf(y) <= (1.f / 3.f) ? fatanh_third(y) : mul(0.5f, __logf(mul(add(1.f, y), frcp(sub(1.f, y)))));
+    return fabsf(y) <= (1.f / 3.f) ? fatanh_third(y) : mul(0.5f, flog(mul(add(1.f, y), frcp(sub(1.f, y)))));
 }
 
-/* log(1 + t)/2 for t >= 0: atanh(t/(2 + t)) by fatanh_third for t <= 1, __logf above
- * (1 + t >= 2, where it is good to a few ulp). */
+/* log(1 + t)/2 for t >= 0: atanh(t/(2 + t)) by fatanh_third for t <= 1, flog above
+ * (1 + t >= 2, where flog is good to a few ulp). */
 __device__ __forceinline__ float half_log1p_pos(float t)
 {
     using namespace f32;
-    return t <= 1.f ? fatanh_third(mul(t, frcp(add(2.f, t)))) : mul(0.5f, __logf(add(1.f, t)));
+    return t <= 1.f ? fatanh_third(mul(t, frcp(add(2.f, t)))) : mul(0.5f, flog(add(1.f, t)));
 }
 
 struct KG32 {
@@ -187,7 +211,7 @@ __device__ __forceinline__ Nie32 nie32(const lt_rec32 &h, float u, float v)
     n.vv = mul(v, v);
     if (TYPE == 5) {
         n.B = fma(h.q2, n.uu, mul(h.k, n.vv)); /* R^2 = (1-e) u^2 + (1+e) v^2 */
-        n.ipc = rsqrtf(n.B);
+        n.ipc = frsqrt(n.B);
         n.pc = mul(n.B, n.ipc);
         n.pt = n.ipt = n.dpsi = 0.f;
         return n;
@@ -203,8 +227,8 @@ __device__ __forceinline__ Nie32 nie32(const lt_rec32 &h, float u, float v)
         return n;
     }
     const float pc2 = add(n.B, h.q2sc2), pt2 = add(n.B, h.q2st2);
-    n.ipc = rsqrtf(pc2);
-    n.ipt = rsqrtf(pt2);
+    n.ipc = frsqrt(pc2);
+    n.ipt = frsqrt(pt2);
     n.pc = mul(pc2, n.ipc);
     n.pt = mul(pt2, n.ipt);
     n.dpsi = mul(h.dq2s2, frcp(add(n.pc, n.pt)));
@@ -284,10 +308,10 @@ __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v, cons
         return sub(xa, mul(h.Asc, log1pf(tc)));
     }
     /* core term: outside the FP64 disc (3 rc and more from the centre) t_c > 2, where
-     * __logf(1 + t) is good to a few ulp, on a term that carries rc << rcut */
+     * flog(1 + t) is good to a few ulp, on a term that carries rc << rcut */
     const float tc = mul(fma(mul(h.tsc, n.B), frcp(add(n.pc, h.qsc)), r2), h.i4rc2);
     const float tt = mul(fma(mul(h.tst, n.B), frcp(add(n.pt, h.qst)), r2), h.i4rcut2);
-    return sub(xa, fma(h.Asc, __logf(add(1.f, tc)), mul(-2.f * h.Ast, half_log1p_pos(tt))));
+    return sub(xa, fma(h.Asc, flog(add(1.f, tc)), mul(-2.f * h.Ast, half_log1p_pos(tt))));
 }
 
 } // namespace lt

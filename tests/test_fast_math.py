@@ -96,3 +96,32 @@ def test_fp32_atanh_third():
     th = _fast_math32(L, s, np.ones_like(s))[3]
     ref = np.arctanh(s.astype(np.float64))
     assert np.max(np.abs(th.astype(np.float64) - ref) / np.abs(ref)) <= 2.4e-7
+
+
+def test_fp32_approx_rcp_rsqrt_log():
+    """The approximate FP32 reciprocal, reciprocal square root and logarithm of the pair
+    loops (the .ftz instruction forms) over normal operands from 1e-30 to 1e30: reciprocal
+    and reciprocal square root within 2^-22 relative of the FP64 values, the logarithm (on
+    its domain in the loops, x >= 2) within 3e-7 relative of FP64 log and of CUDA's logf."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no GPU")
+    from lenstool_hpc_b200 import build
+    build.build()
+    L = lt.load_library()
+    fp = C.POINTER(C.c_float)
+    L.lt_eval_approx32.argtypes = [C.c_int, C.c_int, fp, fp, fp, fp, fp]
+    rng = np.random.default_rng(4)
+    x = np.concatenate([10.0 ** rng.uniform(-30, 30, 300000), rng.uniform(2., 4., 100000),
+                        np.array([1., 2., 3., 4., 1e30])]).astype(np.float32)
+    outs = [np.empty(x.size, np.float32) for _ in range(4)]
+    ptr = lambda a: a.ctypes.data_as(fp)  # noqa: E731
+    assert L.lt_eval_approx32(0, x.size, ptr(x), *[ptr(o) for o in outs]) == 0
+    rcp, rsq, lg, lg_cuda = (o.astype(np.float64) for o in outs)
+    xd = x.astype(np.float64)
+    assert np.max(np.abs(rcp * xd - 1.)) <= 2. ** -22
+    assert np.max(np.abs(rsq * np.sqrt(xd) - 1.)) <= 2. ** -22
+    dom = xd >= 2.
+    ref = np.log(xd[dom])
+    assert np.max(np.abs(lg[dom] - ref) / ref) <= 3e-7
+    assert np.max(np.abs(lg[dom] - lg_cuda[dom]) / ref) <= 3e-7
