@@ -28,20 +28,12 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
 #pragma unroll 1
     for (int h = 0; h < count; h++) {
         const lt_rec64 &r = recs[h];
-        /* OP_NI: the staged records are the closed-form records lt_nie64 */
-        const lt_nie64 &rn = reinterpret_cast<const lt_nie64 &>(r);
-        const double w = kmap ? ((OP & OP_NI) ? rn.w : r.w) : 1.0;
+        const double w = kmap ? r.w : 1.0;
 #pragma unroll
         for (int k = 0; k < P; k++) {
             if ((OP & OP_GRAD) && (OP & OP_GFX)) grad_pair_fast<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
             if ((OP & OP_GRAD) && !(OP & OP_GFX)) grad_pair<TYPE>(r, px[k], py, acc.gx[k], acc.gy[k]);
-            if ((OP & OP_HESS) && (OP & OP_NI)) {
-                const Hess64 t = nie_hess64<TYPE>(rn, px[k], py, w);
-                acc.hxx[k] = __dadd_rn(acc.hxx[k], t.xx);
-                acc.hyy[k] = __dadd_rn(acc.hyy[k], t.yy);
-                acc.hxy[k] = __dadd_rn(acc.hxy[k], t.xy);
-            }
-            if ((OP & OP_HESS) && !(OP & OP_NI)) {
+            if (OP & OP_HESS) {
                 Hess64 hh = {acc.hxx[k], acc.hyy[k], acc.hxy[k]};
                 hess_pair<TYPE>(r, px[k], py, w, hh);
                 acc.hxx[k] = hh.xx;
@@ -52,6 +44,44 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
             if ((OP & OP_POT) && (OP & OP_PEX)) pot_pair<TYPE>(r, px[k], py, acc.psi[k]);
             if ((OP & OP_POT) && !(OP & OP_PEX)) pot_pair_fast<TYPE>(r, px[k], py, acc.psi[k]);
         }
+    }
+}
+
+/* The FP64 recomputation's sums: the closed-form Hessian (nie_hess64) of one chunk of
+ * lt_nie64 records at Q pixels of arbitrary positions (px[k], py[k]), added to
+ * (hxx, hyy, hxy)[k].  The Q pixels' dependent chains are independent of one another, so
+ * the compiler interleaves them; nie_hess64's pinned rounding keeps each pair's value the
+ * same for any Q and in every kernel. */
+template <int Q, int TYPE>
+__device__ __forceinline__ void eval_nie_q(const lt_nie64 *recs, int count, const double (&px)[Q],
+                                           const double (&py)[Q], int kmap, double (&hxx)[Q], double (&hyy)[Q],
+                                           double (&hxy)[Q])
+{
+#pragma unroll 1
+    for (int h = 0; h < count; h++) {
+        const lt_nie64 &r = recs[h];
+        const double w = kmap ? r.w : 1.0;
+#pragma unroll
+        for (int k = 0; k < Q; k++) {
+            const Hess64 t = nie_hess64<TYPE>(r, px[k], py[k], w);
+            hxx[k] = __dadd_rn(hxx[k], t.xx);
+            hyy[k] = __dadd_rn(hyy[k], t.yy);
+            hxy[k] = __dadd_rn(hxy[k], t.xy);
+        }
+    }
+}
+
+/* eval_nie_q over one staged chunk of any profile type. */
+template <int Q>
+__device__ __forceinline__ void eval_nie_chunk(const lt_chunk &c, const lt_nie64 *recs, const double (&px)[Q],
+                                               const double (&py)[Q], int kmap, double (&hxx)[Q],
+                                               double (&hyy)[Q], double (&hxy)[Q])
+{
+    switch (c.type) {
+    case 81: eval_nie_q<Q, 81>(recs, c.count, px, py, kmap, hxx, hyy, hxy); break;
+    case 8: eval_nie_q<Q, 8>(recs, c.count, px, py, kmap, hxx, hyy, hxy); break;
+    case 5: eval_nie_q<Q, 5>(recs, c.count, px, py, kmap, hxx, hyy, hxy); break;
+    default: break;
     }
 }
 

@@ -25,7 +25,7 @@ constexpr int kThreads = 256;
 template <int OP, int P, bool LIST, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a)
 {
-    static_assert(!LIST || P == 1, "list mode evaluates one pixel per thread");
+    static_assert(!LIST || (OP == (OP_HESS | OP_NI)), "list mode: the FP64 recomputation's Hessian");
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[2];
     lt_rec64 *buf0 = reinterpret_cast<lt_rec64 *>(smem);
@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
     if (LIST) {
         nlist = *a.list_count;
         nlist = nlist < a.list_cap ? nlist : a.list_cap;
-        ntiles = (nlist + kThreads - 1) / kThreads;
+        ntiles = (nlist + kThreads * P - 1) / (kThreads * P);
     }
     const int my_tiles = ((int)blockIdx.x < ntiles) ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const long steps = (long)my_tiles * a.nchunks;
@@ -69,30 +69,39 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
     Acc64<OP, P> acc;
     double px[P], py = 0.;
     int ix = 0, iy = 0;
+    double lpy[P];     /* list mode: each pixel's own row coordinate */
+    int lx[P], ly[P];  /* list mode: each pixel's column and row (ly >= ny: no pixel) */
 
     for (long s = 0; s < steps; s++) {
         const int ci = (int)(s % a.nchunks);
         if (ci == 0) {
             const int tile = blockIdx.x + (int)(s / a.nchunks) * gridDim.x;
             if (LIST) {
-                const int e = tile * kThreads + tid;
-                const int p = a.list[e < nlist ? e : nlist - 1];
-                ix = p % a.nx;
-                iy = e < nlist ? p / a.nx : a.ny; /* rows >= ny are not stored */
+                /* P list entries a thread, kThreads apart */
+#pragma unroll
+                for (int k = 0; k < P; k++) {
+                    const int e = (tile * P + k) * kThreads + tid;
+                    const int p = a.list[e < nlist ? e : nlist - 1];
+                    lx[k] = p % a.nx;
+                    ly[k] = e < nlist ? p / a.nx : a.ny; /* rows >= ny are not stored */
+                    px[k] = pixel_x(a, lx[k]);
+                    lpy[k] = pixel_y(a, ly[k] < a.ny ? ly[k] : a.ny - 1);
+                    acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = 0.;
+                }
             } else {
                 const int tx = tile % a.tiles_x, ty = tile / a.tiles_x;
                 ix = tx * kTileW + ox;
                 iy = ty * 8 + oy;
-            }
-            const int cy = iy < a.ny ? iy : a.ny - 1;
-            py = pixel_y(a, cy);
+                const int cy = iy < a.ny ? iy : a.ny - 1;
+                py = pixel_y(a, cy);
 #pragma unroll
-            for (int k = 0; k < P; k++) {
-                const int cx = (ix + k) < a.nx ? ix + k : a.nx - 1;
-                px[k] = pixel_x(a, cx);
-                acc.gx[k] = acc.gy[k] = acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
-                acc.run[k].a = acc.run[k].b = acc.run[k].c = acc.run[k].d = 0.;
-                acc.tot[k].a = acc.tot[k].b = acc.tot[k].c = acc.tot[k].d = 0.;
+                for (int k = 0; k < P; k++) {
+                    const int cx = (ix + k) < a.nx ? ix + k : a.nx - 1;
+                    px[k] = pixel_x(a, cx);
+                    acc.gx[k] = acc.gy[k] = acc.hxx[k] = acc.hyy[k] = acc.hxy[k] = acc.psi[k] = 0.;
+                    acc.run[k].a = acc.run[k].b = acc.run[k].c = acc.run[k].d = 0.;
+                    acc.tot[k].a = acc.tot[k].b = acc.tot[k].c = acc.tot[k].d = 0.;
+                }
             }
         }
         if (tid == 0 && s + 1 < steps) issue(s + 1);
@@ -108,6 +117,23 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
 
         const lt_chunk c = a.chunks[ci];
         const lt_rec64 *recs = b ? buf1 : buf0;
+        if (LIST) {
+            /* the staged records are the closed-form records lt_nie64 */
+            eval_nie_chunk<P>(c, reinterpret_cast<const lt_nie64 *>(recs), px, lpy, a.kmap, acc.hxx, acc.hyy,
+                              acc.hxy);
+            if (ci == a.nchunks - 1) {
+#pragma unroll
+                for (int k = 0; k < P; k++) {
+                    if (ly[k] >= a.ny) continue;
+                    const long pix = (long)ly[k] * a.nx + lx[k];
+                    for (int o = 0; o < a.nout; o++)
+                        a.out[o][pix] = map_value4(a.kinds[o], 0., 0., acc.hxx[k], acc.hyy[k], acc.hxy[k],
+                                                   acc.hxy[k], 0., a.D, a.mult, a.scale);
+                }
+            }
+            __syncthreads(); /* buffer b is refilled by the copy issued at step s + 1 */
+            continue;
+        }
         switch (c.type) {
         case 81: eval_chunk64<OP, P, 81>(recs, c.count, px, py, a.kmap, acc); break;
         case 8: eval_chunk64<OP, P, 8>(recs, c.count, px, py, a.kmap, acc); break;
@@ -183,7 +209,7 @@ int launch_grid64(int op, const GridArgs &args, int num_sms, void *stream, bool 
     cudaStream_t s = (cudaStream_t)stream;
     if (list_mode) { /* the FP32C recomputation pass: the out-of-line fast Hessian */
         if (op != OP_HESS) return (int)cudaErrorInvalidValue;
-        return launch_op<OP_HESS | OP_NI, 1, true, 2>(args, num_sms, s);
+        return launch_op<OP_HESS | OP_NI, 2, true, 2>(args, num_sms, s);
     }
     switch (op) {
     case OP_GRAD: return launch_shape<OP_GRAD>(shape, args, num_sms, s);

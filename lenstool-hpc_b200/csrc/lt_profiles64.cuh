@@ -545,46 +545,53 @@ __device__ __forceinline__ void hess_pair(const lt_rec64 &h, double px, double p
 /* The sky-frame Hessian of one pair from the real-valued closed form (lt_profiles32.cuh's
  * forms in FP64, record lt_nie64), weight w included: the FP32C path's recomputation of
  * pixels near critical curves.  About 60 FP64 operations for a dPIE pair against ~95 for
- * the reference's quotient form, and no 0/0 point; equal to it within ~1e-15 of the terms. */
+ * the reference's quotient form, and no 0/0 point; equal to it within ~1e-15 of the terms.
+ * Every operation's rounding is pinned (explicit round-to-nearest multiply, add and fused
+ * multiply-add), so the function can be inlined into any kernel, and interleaved over
+ * several pixels, and still round each pair alike everywhere. */
 template <int TYPE>
-__device__ __noinline__ Hess64 nie_hess64(const lt_nie64 &h, double px, double py, double w)
+__device__ __forceinline__ Hess64 nie_hess64(const lt_nie64 &h, double px, double py, double w)
 {
-    const double tx = px - h.x0, ty = py - h.y0;
-    const double u = tx * h.cs + ty * h.sn, v = ty * h.cs - tx * h.sn;
-    const double uu = u * u, vv = v * v;
+    using ex::A;
+    using ex::M;
+    using ex::S;
+    const double tx = S(px, h.x0), ty = S(py, h.y0);
+    const double u = __fma_rn(tx, h.cs, M(ty, h.sn)), v = __fma_rn(ty, h.cs, -M(tx, h.sn));
+    const double uu = M(u, u), vv = M(v, v), uv = M(u, v);
     double k, g1, g2;
     if (TYPE == 5) {
-        const double ir = rsqrt64(h.q2 * uu + h.k * vv);
-        const double kk = h.K * ir * ir * ir;
-        k = 0.5 * kk * (uu + vv);
-        g1 = 0.5 * kk * (vv - uu);
-        g2 = -kk * u * v;
+        const double ir = rsqrt64(__fma_rn(h.q2, uu, M(h.k, vv)));
+        const double kk = M(M(h.K, ir), M(ir, ir));
+        const double hk = M(0.5, kk);
+        k = M(hk, A(uu, vv));
+        g1 = M(hk, S(vv, uu));
+        g2 = M(-kk, uv);
     } else {
-        const double B = h.q2 * uu + vv, r2 = uu + vv;
-        const double pc2 = B + h.q2sc2;
-        const double ipc = rsqrt64(pc2), pc = pc2 * ipc;
-        const double Dc = h.tsc * pc + (h.opsc2 + r2);
+        const double B = __fma_rn(h.q2, uu, vv), r2 = A(uu, vv);
+        const double pc2 = A(B, h.q2sc2);
+        const double ipc = rsqrt64(pc2), pc = M(pc2, ipc);
+        const double Dc = __fma_rn(h.tsc, pc, A(h.opsc2, r2));
         if (TYPE == 8) {
-            const double E = ipc * rcp64(Dc);
-            k = h.K * ipc;
-            g1 = h.Kc1sc2 * E + h.K * (vv - uu) * E;
-            g2 = -2. * h.K * u * v * E;
+            const double E = M(ipc, rcp64(Dc));
+            k = M(h.K, ipc);
+            g1 = __fma_rn(h.Kc1sc2, E, M(M(h.K, S(vv, uu)), E));
+            g2 = M(M(-2. * h.K, uv), E);
         } else {
-            const double pt2 = B + h.q2st2;
-            const double ipt = rsqrt64(pt2), pt = pt2 * ipt;
-            const double Dt = h.tst * pt + (h.opst2 + r2);
-            const double dpsi = h.dq2s2 * rcp64(pc + pt);
-            const double dD = 2. * (pt * h.ds + h.sc * dpsi) + h.opds2;
-            const double dpD = dpsi * Dc + pt * dD;
-            const double Ec = ipc * rcp64(Dc), Et = ipt * rcp64(Dt);
-            const double dEK = -h.K * (dpD * Ec) * Et;
-            k = -h.K * dpsi * (ipc * ipt);
-            g1 = h.Kc1sc2 * Ec - h.Kc1st2 * Et + (vv - uu) * dEK;
-            g2 = -2. * (u * v) * dEK;
+            const double pt2 = A(B, h.q2st2);
+            const double ipt = rsqrt64(pt2), pt = M(pt2, ipt);
+            const double Dt = __fma_rn(h.tst, pt, A(h.opst2, r2));
+            const double dpsi = M(h.dq2s2, rcp64(A(pc, pt)));
+            const double dD = __fma_rn(2., __fma_rn(pt, h.ds, M(h.sc, dpsi)), h.opds2);
+            const double dpD = __fma_rn(dpsi, Dc, M(pt, dD));
+            const double Ec = M(ipc, rcp64(Dc)), Et = M(ipt, rcp64(Dt));
+            const double dEK = M(M(-h.K, M(dpD, Ec)), Et);
+            k = M(M(-h.K, dpsi), M(ipc, ipt));
+            g1 = __fma_rn(h.Kc1sc2, Ec, __fma_rn(-h.Kc1st2, Et, M(S(vv, uu), dEK)));
+            g2 = M(-2., M(uv, dEK));
         }
     }
-    const double gs1 = g1 * h.c2t - g2 * h.s2t, gs2 = g1 * h.s2t + g2 * h.c2t;
-    return {w * (k + gs1), w * (k - gs1), w * gs2};
+    const double gs1 = __fma_rn(g1, h.c2t, -M(g2, h.s2t)), gs2 = __fma_rn(g1, h.s2t, M(g2, h.c2t));
+    return {M(w, A(k, gs1)), M(w, S(k, gs1)), M(w, gs2)};
 }
 
 /* The FP64 terms of one pair as out-of-line functions, for the FP32C path's FP64 work (its

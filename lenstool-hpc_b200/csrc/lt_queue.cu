@@ -285,36 +285,40 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
     }
     if (!recompute) return true;
     __syncthreads();
+    /* the flagged pixels (at most the tile's 32 P x 8 = P kQThreads): P a thread, in one
+     * walk of the catalogue's FP64 closed-form records */
     const int n = *s_count;
     const int tile_x0 = (tile % a.tiles_x) * 32 * P, tile_y0 = (tile / a.tiles_x) * 8;
-    for (int base = 0; base < n; base += kQThreads) {
-        const int e = base + (int)threadIdx.x;
-        const bool have = e < n;
-        const int l = have ? s_list[e] : 0;
-        const int qx = tile_x0 + l % (32 * P), qy = tile_y0 + l / (32 * P);
-        double qpx[1] = {pixel_x(a, have ? qx : 0)};
-        const double qpy = pixel_y(a, have ? qy : 0);
-        Acc64<OP_HESS | OP_NI, 1> h;
-        h.hxx[0] = h.hyy[0] = h.hxy[0] = 0.;
-        ok = walk_chunks(st, a.chunks, a.nchunks, reinterpret_cast<const lt_rec64 *>(it.nie64), nullptr, status,
-                         [&](const lt_chunk &c, const unsigned char *buf) {
-                             if (!have) return;
-                             const lt_rec64 *recs = reinterpret_cast<const lt_rec64 *>(buf);
-                             switch (c.type) {
-                             case 81: eval_chunk64<OP_HESS | OP_NI, 1, 81>(recs, c.count, qpx, qpy, a.kmap, h); break;
-                             case 8: eval_chunk64<OP_HESS | OP_NI, 1, 8>(recs, c.count, qpx, qpy, a.kmap, h); break;
-                             case 5: eval_chunk64<OP_HESS | OP_NI, 1, 5>(recs, c.count, qpx, qpy, a.kmap, h); break;
-                             default: break;
-                             }
-                         });
-        if (!ok) return false;
-        if (have) {
-            const long p = (long)qy * a.nx + qx;
-            for (int o = 0; o < a.nout; o++) {
-                const int kind = a.kinds[o];
-                if (is_grad_kind(kind) || kind == KIND_POT) continue;
-                a.out[o][p] = map_value(kind, 0., 0., h.hxx[0], h.hyy[0], h.hxy[0], 0., a.D, a.mult, a.scale);
-            }
+    if (n == 0) return true;
+    bool have[P];
+    int qx[P], qy[P];
+    double qpx[P], qpy[P], hxx[P], hyy[P], hxy[P];
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        const int e = k * kQThreads + (int)threadIdx.x;
+        have[k] = e < n;
+        const int l = have[k] ? s_list[e] : 0;
+        qx[k] = tile_x0 + l % (32 * P);
+        qy[k] = tile_y0 + l / (32 * P);
+        qpx[k] = pixel_x(a, qx[k]);
+        qpy[k] = pixel_y(a, qy[k]);
+        hxx[k] = hyy[k] = hxy[k] = 0.;
+    }
+    const bool ok2 = walk_chunks(st, a.chunks, a.nchunks, reinterpret_cast<const lt_rec64 *>(it.nie64), nullptr,
+                                 status, [&](const lt_chunk &c, const unsigned char *buf) {
+                                     if (!have[0]) return;
+                                     eval_nie_chunk<P>(c, reinterpret_cast<const lt_nie64 *>(buf), qpx, qpy, a.kmap,
+                                                       hxx, hyy, hxy);
+                                 });
+    if (!ok2) return false;
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        if (!have[k]) continue;
+        const long p = (long)qy[k] * a.nx + qx[k];
+        for (int o = 0; o < a.nout; o++) {
+            const int kind = a.kinds[o];
+            if (is_grad_kind(kind) || kind == KIND_POT) continue;
+            a.out[o][p] = map_value(kind, 0., 0., hxx[k], hyy[k], hxy[k], 0., a.D, a.mult, a.scale);
         }
     }
     return true;
