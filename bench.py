@@ -60,9 +60,9 @@ FLOPS_PER_PAIR = 182 + 760
 # says whether the timed build is that one.
 KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
                   "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
-INST_SOURCES_SHA = "e10d46a7870db5c2"
-INST_PER_PAIR_FP32C_LENS = 156.1
-FP32_FLOPS_PER_PAIR_FP32C_LENS = 130.4
+INST_SOURCES_SHA = "598ac6322c48639d"
+INST_PER_PAIR_FP32C_LENS = 150.6
+FP32_FLOPS_PER_PAIR_FP32C_LENS = 126.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
 TRAFFIC_FP32C_LENS_4096 = 14123264 + 633822976
@@ -529,7 +529,13 @@ def bench_chi2(ctx, n_models=64, n=2048, nsys=40, seed=20261203 + 3, cpu=True):
            "models_per_s": n_models / dt, "ms_per_model": 1e3 * dt / n_models,
            "seconds_for_4096_models": 4096 * dt / n_models, "deflection_evals_per_s": n_models * n * n * base.n / dt,
            "chi2_true_model": true_chi, "chi2_median_perturbed": float(np.median(chi))}
-    # the deflection grid in LT_FP32C, delensing and chi2 in FP64
+    # the deflection grid in LT_FP64_FAST (within 2e-12 of the reference's arithmetic), then in
+    # LT_FP32C; delensing and chi2 in FP64
+    dtf, (chif, foundf) = timed("fp64fast")
+    res["fp64fast_deflections"] = {
+        "models_per_s": n_models / dtf, "ms_per_model": 1e3 * dtf / n_models,
+        "same_images_found": bool(np.array_equal(foundf, found)),
+        "max_rel_chi2_diff": float(np.max(np.abs(chif - chi) / np.maximum(np.abs(chi), 1.)))}
     dt32, (chi32, found32) = timed("fp32c")
     res["fp32c_deflections"] = {
         "models_per_s": n_models / dt32, "ms_per_model": 1e3 * dt32 / n_models,

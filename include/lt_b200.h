@@ -477,8 +477,8 @@ uint64_t lt_kernel_launch_count(void);
 double lt_measure_fma_peak(int fp32, int device);
 
 /* Evaluate, on `device`, the reciprocal and reciprocal square root that the FP64 pair
- * loops use for their per-pair denominators (hardware approximation + two Newton-Raphson
- * steps) on n host inputs: a diagnostic for the tests (0 = LT_OK).  No counterpart in the
+ * loops use for their per-pair denominators (hardware approximation + one third-order
+ * refinement) on n host inputs: a diagnostic for the tests (0 = LT_OK).  No counterpart in the
  * reference. */
 int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt);
 

@@ -138,7 +138,8 @@ EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release",
            "lt_server_create",
            "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
            "lt_server_get_stats", "lt_server_destroy", "lt_chi2", "lt_chi2_batch", "lt_delense",
-           "lt_catalog_update", "lt_write_fits", "lt_eval_fast_math", "lt_eval_fast_math32", "lt_eval_approx32",
+           "lt_catalog_update", "lt_write_fits", "lt_eval_fast_math", "lt_eval_fast_math32",
+           "lt_eval_approx32",
            "lt_bayes_create",
            "lt_bayes_apply", "lt_bayes_destroy", "lt_chi2_batch_precision", "lt_server_submit_chi2",
            "lt_server_chi2_result", "lt_server_inject_fault")

@@ -213,6 +213,7 @@ LT_HD inline void pack32(const lt_rec64 &r, int type, int idx64, lt_rec32 &o)
     o.q2sc = f32(mul(q2, sc));
     o.q2st = f32(mul(q2, st));
     o.Asc = f32(mul(0.5, mul(A, sc)));
+    o.Ascl2 = f32(mul(mul(0.5, mul(A, sc)), 0.69314718055994530942));
     o.Ast = f32(mul(0.5, mul(A, st)));
     o.i4rc2 = f32(div(1., mul(4., mul(r.rc, r.rc))));
     o.i4rcut2 = f32(div(1., mul(4., mul(r.rcut, r.rcut))));

@@ -79,9 +79,8 @@ __global__ void fast_math_kernel(const double *x, double *rcp, double *rsq, int 
         rsq[i] = lt::rsqrt64(x[i]);
     }
 }
-} // namespace
 
-extern "C" int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt)
+int eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt)
 {
     if (n < 1 || !x || !rcp || !rsqrt) return 1;
     if (cudaSetDevice(device) != cudaSuccess) return 4;
@@ -97,6 +96,12 @@ extern "C" int lt_eval_fast_math(int device, int n, const double *x, double *rcp
     if (e == cudaSuccess) e = cudaMemcpy(rsqrt, d + 2 * n, b, cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? 0 : 4;
+}
+} // namespace
+
+extern "C" int lt_eval_fast_math(int device, int n, const double *x, double *rcp, double *rsqrt)
+{
+    return eval_fast_math(device, n, x, rcp, rsqrt);
 }
 
 /* ---- the FP32 atan2 and square root of the compensated pair loops (lt_profiles32.cuh) ---- */

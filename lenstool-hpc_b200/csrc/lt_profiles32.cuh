@@ -56,7 +56,7 @@ struct alignas(16) lt_rec32 {
     float q2st, Asc, Ast, i4rc2;     /* q^2 s_t, A s_c/2, A s_t/2, 1/(4 rc^2)                 */
     float i4rcut2;                   /* 1/(4 rcut^2)                                          */
     int32_t type, idx64;
-    float pad;
+    float Ascl2;                     /* A s_c ln(2)/2                                         */
 };
 static_assert(sizeof(lt_rec32) == 160, "record size");
 
@@ -97,14 +97,19 @@ __device__ __forceinline__ float frsqrt(float x)
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
-/* Natural logarithm as ln 2 log2(x) for x >= 2 (where the log2 instruction's absolute error
- * is a few ulp of the result). */
-__device__ __forceinline__ float flog(float x)
+/* log2 by the approximate instruction; the natural logarithm as ln 2 log2(x) and half of it
+ * as (ln 2 / 2) log2(x), for x >= 2 (where the log2 instruction's absolute error is a few
+ * ulp of the result).  ln 2 / 2 in FP32 is exactly half of ln 2 in FP32, so the half
+ * logarithm is exactly half of flog's value (one multiply instead of two). */
+__device__ __forceinline__ float flog2(float x)
 {
     float r;
     asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return __fmul_rn(r, 0.693147182f);
+    return r;
 }
+constexpr float kLn2f = 0.693147182f, kHalfLn2f = 0.346573591f;
+__device__ __forceinline__ float flog(float x) { return __fmul_rn(flog2(x), kLn2f); }
+__device__ __forceinline__ float fhalf_log(float x) { return __fmul_rn(flog2(x), kHalfLn2f); }
 
 /* Square root to the approximate instruction's accuracy (relative error ~2^-23), for
  * operands whose rounding the compensated path tolerates; zero and denormals give 0. */
@@ -176,7 +181,7 @@ __device__ __forceinline__ float fatanh_third(float s)
 __device__ __forceinline__ float fatanh_any(float y)
 {
     using namespace f32;
-    return fabsf(y) <= (1.f / 3.f) ? fatanh_third(y) : mul(0.5f, flog(mul(add(1.f, y), frcp(sub(1.f, y)))));
+    return fabsf(y) <= (1.f / 3.f) ? fatanh_third(y) : fhalf_log(mul(add(1.f, y), frcp(sub(1.f, y))));
 }
 
 /* log(1 + t)/2 for t >= 0: atanh(t/(2 + t)) by fatanh_third for t <= 1, flog above
@@ -184,7 +189,7 @@ __device__ __forceinline__ float fatanh_any(float y)
 __device__ __forceinline__ float half_log1p_pos(float t)
 {
     using namespace f32;
-    return t <= 1.f ? fatanh_third(mul(t, frcp(add(2.f, t)))) : mul(0.5f, flog(add(1.f, t)));
+    return t <= 1.f ? fatanh_third(mul(t, frcp(add(2.f, t)))) : fhalf_log(add(1.f, t));
 }
 
 struct KG32 {
@@ -295,7 +300,8 @@ __device__ __forceinline__ G32 grad32(const lt_rec32 &h, float u, float v, const
 
 /* Potential of one pair from its deflection g (halo frame):
  *   u g_x + v g_y - (A s_c/2) log(1 + t_c) [+ (A s_t/2) log(1 + t_t) for the dPIE],
- *   t_s = (u^2 + v^2 + 2 s B/(psi_s + q s)) / (4 r^2), a sum of non-negative terms. */
+ *   t_s = (u^2 + v^2 + 2 s B/(psi_s + q s)) / (4 r^2), a sum of non-negative terms,
+ *   1 + t_s = ((psi_s + s)^2 + k^2 u^2) / (4 r^2). */
 template <int TYPE>
 __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v, const Nie32 &n, const G32 &g)
 {
@@ -307,11 +313,14 @@ __device__ __forceinline__ float pot32(const lt_rec32 &h, float u, float v, cons
         const float tc = mul(add(r2, __fdiv_rn(mul(h.tsc, n.B), add(n.pc, h.qsc))), h.i4rc2);
         return sub(xa, mul(h.Asc, log1pf(tc)));
     }
-    /* core term: outside the FP64 disc (3 rc and more from the centre) t_c > 2, where
-     * flog(1 + t) is good to a few ulp, on a term that carries rc << rcut */
-    const float tc = mul(fma(mul(h.tsc, n.B), frcp(add(n.pc, h.qsc)), r2), h.i4rc2);
+    /* core term: outside the FP64 disc (3 rc and more from the centre) t_c > 2, so 1 + t_c
+     * is taken directly as ((psi_c + s_c)^2 + k^2 u^2) / (4 rc^2), a sum of non-negative
+     * terms with psi_c + s_c shared with the deflection, and log2 of it is good to a few
+     * ulp; on a term that carries rc << rcut */
+    const float pcs = add(n.pc, h.sc);
+    const float opt_c = mul(fma(h.k2, n.uu, mul(pcs, pcs)), h.i4rc2);
     const float tt = mul(fma(mul(h.tst, n.B), frcp(add(n.pt, h.qst)), r2), h.i4rcut2);
-    return sub(xa, fma(h.Asc, flog(add(1.f, tc)), mul(-2.f * h.Ast, half_log1p_pos(tt))));
+    return sub(xa, fma(h.Ascl2, flog2(opt_c), mul(-2.f * h.Ast, half_log1p_pos(tt))));
 }
 
 } // namespace lt

@@ -19,29 +19,28 @@
 namespace lt {
 
 /* Reciprocal and reciprocal square root for the per-pair denominators: the hardware
- * approximations (rcp.approx.ftz.f64, rsqrt.approx.ftz.f64) refined by two Newton-Raphson
- * steps, y <- y + y (1 - x y) and y <- y + (y/2)(1 - x y^2); each step doubles the number of
- * correct bits, so the result is within a few ulp of the correctly rounded value for
- * positive normal inputs (checked against 1/x and 1/sqrt(x) by the tests).  Four FMAs
- * and one approximation instead of the IEEE division / square-root sequences. */
+ * approximations (rcp.approx.ftz.f64, rsqrt.approx.ftz.f64; ~20 correct bits) refined by one
+ * third-order step: with e = 1 - x y, 1/x = y/(1 - e) = y (1 + e + e^2 + O(e^3)); with
+ * h = 1 - x y^2, 1/sqrt(x) = y (1 - h)^(-1/2) = y (1 + h/2 + 3 h^2/8 + O(h^3)).  The
+ * truncation is ~e^3 (~1e-18), so the result is within a few ulp of the correctly rounded
+ * value for positive normal inputs (checked against 1/x and 1/sqrt(x) by the tests).
+ * Three FP64 operations for a reciprocal and five for a reciprocal square root (two
+ * Newton steps take four and eight), and one approximation, instead of the IEEE division
+ * and square-root sequences. */
 __device__ __forceinline__ double rcp64(double x)
 {
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-x, y, 1.0);
-    return fma(y, e, y);
+    const double e = fma(-x, y, 1.0);
+    return fma(y, fma(e, e, e), y);
 }
 
 __device__ __forceinline__ double rsqrt64(double x)
 {
     double y;
     asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double h = fma(-x * y, y, 1.0);
-    y = fma(0.5 * y, h, y);
-    h = fma(-x * y, y, 1.0);
-    return fma(0.5 * y, h, y);
+    const double h = fma(-x * y, y, 1.0);
+    return fma(y * h, fma(0.375, h, 0.5), y);
 }
 
 struct Frame64 {
@@ -544,7 +543,7 @@ __device__ __forceinline__ void hess_pair(const lt_rec64 &h, double px, double p
 
 /* The sky-frame Hessian of one pair from the real-valued closed form (lt_profiles32.cuh's
  * forms in FP64, record lt_nie64), weight w included: the FP32C path's recomputation of
- * pixels near critical curves.  About 60 FP64 operations for a dPIE pair against ~95 for
+ * pixels near critical curves.  About 70 FP64 operations for a dPIE pair against ~95 for
  * the reference's quotient form, and no 0/0 point; equal to it within ~1e-15 of the terms.
  * Every operation's rounding is pinned (explicit round-to-nearest multiply, add and fused
  * multiply-add), so the function can be inlined into any kernel, and interleaved over

@@ -1,6 +1,6 @@
 """The FP64 reciprocal and reciprocal square root of the pair loops (hardware
-approximation refined by two Newton-Raphson steps) against the correctly rounded
-1/x and 1/sqrt(x), over the input range of the per-pair denominators."""
+approximation refined by one third-order step) against the correctly rounded 1/x and
+1/sqrt(x), over the input range of the per-pair denominators."""
 import ctypes as C
 
 import numpy as np
