@@ -276,6 +276,7 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
         post.apply(rows_dev, cats, stream)
         batch.launch(stream)
     ctx.synchronize(stream)
+    ctx.recompute_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n0 = lt.launch_count()
     e0.record(stream)
@@ -286,12 +287,15 @@ def bench_posterior_batch(ctx, precision, steps, warmup, n_sets=512, plain_sampl
     ctx.synchronize(stream)
     launches = lt.launch_count() - n0
     dt = e0.elapsed_time(e1) / 1e3 / steps
+    recomputed = ctx.recompute_count()
+    npix_all = float(sum(int(n) * int(n) for n in sizes)) * steps
     res = {"workload": f"posterior_batch: {n_sets} bayes rows x {base.n} halos, grids U{{512,1024,2048}}^2, "
                        f"mu+kappa", "precision": precision, "maps_per_s": 2 * n_sets / dt, "sets_per_s": n_sets / dt,
            "evals_per_s": evals / dt, "ms_per_step": dt * 1e3, "gpu_launches_per_step": launches / steps,
            "evals_per_step": evals, "l2": f"outputs {2 * 8 * evals / base.n / 1e9:.1f} GB per step > L2",
            "step": "lt_bayes_apply of the rows (HBM) + one lt_batch graph",
-           "shape": dict(batch.config(), autotuned=tune)}
+           "shape": dict(batch.config(), autotuned=tune),
+           "pixels_recomputed_fp64": recomputed / npix_all}
     # the sets as host catalogues (the reference's host-side row update), for the plain loop
     plain_sample = min(plain_sample, n_sets)
     sets = [bayes.catalog_from_state(model, bayes.reference_state(model, (), cols, rows[i]))
@@ -660,6 +664,7 @@ def main():
     if timing:
         ctx.set_pass_timing(True)
         ctx.pass_times()
+        ctx.recompute_count()
     barrier()
     n0 = lt.launch_count()
     with ClockSampler(gpu_id) as clocks:
@@ -678,7 +683,9 @@ def main():
     if timing:
         p1, p2, ncalls = ctx.pass_times()
         ctx.set_pass_timing(False)
-        passes = {"pass1_ms": p1 / max(ncalls, 1), "pass2_ms": p2 / max(ncalls, 1), "calls": ncalls}
+        recomputed = ctx.recompute_count()
+        passes = {"pass1_ms": p1 / max(ncalls, 1), "pass2_ms": p2 / max(ncalls, 1), "calls": ncalls,
+                  "pixels_recomputed_fp64": recomputed / float(g.npix * args.steps)}
     evals_step = sums_per_pair * g.npix * cat.n
     value, elapsed, _ = replicas.throughput(evals_step * args.steps, elapsed, "cuda")
 

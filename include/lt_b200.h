@@ -290,6 +290,11 @@ lt_status lt_autotune(lt_context *ctx, const lt_catalog *cat, int32_t precision,
 lt_status lt_set_pass_timing(lt_context *ctx, int32_t on);
 lt_status lt_pass_times(lt_context *ctx, double *pass1_ms, double *pass2_ms, int32_t *calls);
 
+/* Pixels of the LT_FP32C calls, batches and serving loops of this context recomputed in
+ * FP64 (their error estimate failed after pass 1) since the previous read; resets the
+ * count.  No counterpart in the reference. */
+lt_status lt_recompute_count(lt_context *ctx, uint64_t *pixels);
+
 /* ---- requests: batches and the serving loop ----------------------------------------
  * A request is one grid of output planes over one uploaded catalogue: any mix of Hessian
  * maps (lt_map_kind 0-41, with `dlsds` as D, `kmap` and `mult` as in lt_hessian_maps),

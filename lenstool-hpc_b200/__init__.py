@@ -133,7 +133,7 @@ EXPORTS = ("lt_create", "lt_destroy", "lt_catalog_upload", "lt_catalog_release",
            "lt_gradient_grid", "lt_hessian_maps", "lt_potential_grid", "lt_lens_maps", "lt_synchronize",
            "lt_cosmo_distances", "lt_kernel_launch_count", "lt_status_string", "lt_last_error", "lt_abi_version",
            "lt_set_kernel_shape", "lt_get_kernel_shape", "lt_set_kernel_config", "lt_get_kernel_config",
-           "lt_autotune", "lt_measure_fma_peak", "lt_set_pass_timing", "lt_pass_times",
+           "lt_autotune", "lt_measure_fma_peak", "lt_set_pass_timing", "lt_pass_times", "lt_recompute_count",
            "lt_batch_create", "lt_batch_launch", "lt_batch_size", "lt_batch_config", "lt_batch_destroy",
            "lt_server_create",
            "lt_server_submit", "lt_server_poll", "lt_server_wait", "lt_server_request_times", "lt_server_release",
@@ -175,6 +175,7 @@ def load_library(path=None):
     L.lt_autotune.argtypes = [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
     L.lt_set_pass_timing.argtypes = [vp, C.c_int32]
     L.lt_pass_times.argtypes = [vp, _dp, _dp, _ip]
+    L.lt_recompute_count.argtypes = [vp, C.POINTER(C.c_uint64)]
     L.lt_measure_fma_peak.argtypes = [C.c_int, C.c_int]
     L.lt_measure_fma_peak.restype = C.c_double
     L.lt_batch_create.argtypes = [vp, C.POINTER(_Request), C.c_int32, C.c_int32, C.POINTER(vp)]
@@ -436,6 +437,12 @@ class Context:
         a, b, n = C.c_double(), C.c_double(), C.c_int32()
         self._check(self._lib.lt_pass_times(self.handle, C.byref(a), C.byref(b), C.byref(n)), "lt_pass_times")
         return a.value, b.value, n.value
+
+    def recompute_count(self):
+        """Pixels of the FP32C calls recomputed in FP64 since the last read (lt_recompute_count)."""
+        a = C.c_uint64()
+        self._check(self._lib.lt_recompute_count(self.handle, C.byref(a)), "lt_recompute_count")
+        return a.value
 
     def synchronize(self, stream=None):
         self._check(self._lib.lt_synchronize(self.handle, _stream_handle(stream)), "lt_synchronize")

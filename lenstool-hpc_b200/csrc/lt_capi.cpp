@@ -354,6 +354,20 @@ lt_status lt_pass_times(lt_context *ctx, double *pass1_ms, double *pass2_ms, int
     return st;
 }
 
+lt_status lt_recompute_count(lt_context *ctx, uint64_t *pixels)
+{
+    if (!ctx || !pixels) return LT_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    uint64_t c = 0;
+    /* words 2..3 of the status block: the 64-bit count that the recomputation kernels add to */
+    cudaError_t e = cudaMemcpy(&c, ctx->status + 2, sizeof(c), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemset(ctx->status + 2, 0, sizeof(c));
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "recompute count");
+    *pixels = c;
+    return LT_OK;
+}
+
 lt_status lt_catalog_upload(lt_context *ctx, const lt_halo_soa *s, lt_catalog **out)
 {
     if (!ctx || !s || !out || s->nhalos < 0) return LT_ERR_INVALID_ARGUMENT;

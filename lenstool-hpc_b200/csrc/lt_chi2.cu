@@ -436,6 +436,9 @@ int chi2_launch(lt_context *ctx, const lt_catalog *cat, Chi2Buf &b, bool sources
         if (err == cudaSuccess) err = (int)cudaMemsetAsync((void *)c.ay, 0, 8 * (size_t)c.n * c.n, s);
     } else if (precision == LT_FP32C) {
         err = launch_fp32c(ctx, cat, OP_GRAD, a, s);
+    } else if (precision == LT_FP64_FAST) {
+        /* the dPIE deflection as log(1 + eps), as the LT_FP64_FAST grid calls take it */
+        err = launch_grid64_tiled(OP_GRAD | OP_GFX, a, ctx->num_sms, s, ctx->shape[LT_FP64_FAST][OP_GRAD]);
     } else {
         err = launch_grid64_tiled(OP_GRAD, a, ctx->num_sms, s, ctx->shape[LT_FP64][OP_GRAD]);
     }

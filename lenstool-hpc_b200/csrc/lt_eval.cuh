@@ -365,7 +365,7 @@ __device__ __forceinline__ void fp32c_grad_total(const Acc32<P> &acc, int k, dou
 /* True when the FP32 part's error bound on the magnification exceeds mu_tol of
  * max(|mu|, 1) (near a critical curve the determinant amplifies the error of the sums):
  * |d mu| = mu^2 |d det| <= mu_tol max(|mu|, 1), i.e. |d det| <= mu_tol |det| max(1, |det|).
- * (A map of mu is judged against max(|mu|, its RMS), and its RMS is at least about 1, the
+ * (A map of mu is measured against max(|mu|, its RMS), and its RMS is at least about 1, the
  * magnification far from any lens.)  The pixel is then recomputed in FP64. */
 __device__ __forceinline__ bool fp32c_flag(double det, double det_err, double mu_tol)
 {

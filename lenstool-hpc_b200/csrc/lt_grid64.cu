@@ -42,6 +42,10 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
         nlist = *a.list_count;
         nlist = nlist < a.list_cap ? nlist : a.list_cap;
         ntiles = (nlist + kThreads * P - 1) / (kThreads * P);
+        /* the count of recomputed pixels (lt_recompute_count): the 64-bit word 2 of the
+         * context's status block */
+        if (blockIdx.x == 0 && tid == 0 && a.status)
+            atomicAdd(reinterpret_cast<unsigned long long *>(a.status + 2), (unsigned long long)nlist);
     }
     const int my_tiles = ((int)blockIdx.x < ntiles) ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
     const long steps = (long)my_tiles * a.nchunks;

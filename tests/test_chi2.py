@@ -105,3 +105,18 @@ def test_chi2_fp32c_deflections(ctx, setup):
         print(n, "found", f64.tolist(), f32.tolist(), "max rel chi2 diff", rel.max())
         assert np.array_equal(f32, f64)
         assert rel.max() <= 1e-3
+
+
+def test_chi2_fp64fast_deflections(ctx, setup):
+    """The deflection grid in LT_FP64_FAST (the dPIE deflection through log(1 + eps), within
+    2e-12 of the reference's arithmetic), the rest as in LT_FP64: the same images found and
+    chi2 within 1e-9 (a deflection change of 1e-12 moves no inclusion test here)."""
+    cat, dcat, s = setup
+    rng = np.random.Generator(np.random.PCG64(10))
+    handles = [dcat] + [ctx.upload(catalog.perturb_catalog(cat, rng)) for _ in range(3)]
+    c64, f64 = ctx.chi2(handles, FRAME, 512, s)
+    cf, ff = ctx.chi2(handles, FRAME, 512, s, precision="fp64fast")
+    rel = np.abs(cf - c64) / np.maximum(np.abs(c64), 1.)
+    print("found", f64.tolist(), ff.tolist(), "max rel chi2 diff", rel.max())
+    assert np.array_equal(ff, f64)
+    assert rel.max() <= 1e-9

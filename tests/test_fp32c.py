@@ -231,3 +231,18 @@ def test_host_outputs_in_bands_equal_device_outputs(ctx, precision):
     ctx.synchronize()
     for k in host:
         assert np.array_equal(host[k], dev[k].cpu().numpy()), (precision, k)
+
+
+def test_recompute_count(ctx):
+    """lt_recompute_count: the pixels a call recomputes in FP64 (its flagged pixels, some of
+    this field's); a call without determinant-sensitive maps recomputes none."""
+    cat, _ = catalog.workload("maps_1000h_4096")
+    g = catalog.Grid.square(150., 512)
+    dcat = ctx.upload(cat)
+    ctx.recompute_count()
+    _maps(ctx, dcat, g, "fp32c")
+    n = ctx.recompute_count()
+    print("recomputed", n, "of", g.npix)
+    assert 0 < n < g.npix
+    _maps(ctx, dcat, g, "fp32c", kinds=("kappa", "gamma1"))
+    assert ctx.recompute_count() == 0
