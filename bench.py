@@ -60,12 +60,12 @@ FLOPS_PER_PAIR = 182 + 760
 # says whether the timed build is that one.
 KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
                   "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
-INST_SOURCES_SHA = "85f727158fc4e270"
+INST_SOURCES_SHA = "7518cb9f271e825f"
 INST_PER_PAIR_FP32C_LENS = 150.6
 FP32_FLOPS_PER_PAIR_FP32C_LENS = 126.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
-TRAFFIC_FP32C_LENS_4096 = 21176576 + 634733824
+TRAFFIC_FP32C_LENS_4096 = 16228864 + 633445888
 
 
 def _package():
