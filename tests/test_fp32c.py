@@ -246,3 +246,26 @@ def test_recompute_count(ctx):
     assert 0 < n < g.npix
     _maps(ctx, dcat, g, "fp32c", kinds=("kappa", "gamma1"))
     assert ctx.recompute_count() == 0
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_fp32c_random_fields_hold_the_bound(ctx, seed):
+    """The error estimate (three standard deviations of the FP32 terms' independent errors,
+    against a tolerance of half the target) over random cluster + galaxy fields of different
+    richness and magnification: kappa, gamma1, gamma2 and mu within 1e-6 of LT_FP64 on a
+    1024^2 grid, pixels with |mu| > 100 excluded."""
+    rng = np.random.default_rng(100 + seed)
+    nc = int(rng.integers(1, 5))
+    ng = int(rng.integers(100, 800))
+    cat = catalog.cluster_galaxy_catalog(nc, ng, 1000 + seed)
+    g = catalog.Grid.square(float(rng.uniform(60., 160.)), 1024)
+    D = float(rng.uniform(0.3, 0.9))
+    dcat = ctx.upload(cat)
+    m64 = _maps(ctx, dcat, g, "fp64", D=D)
+    m32 = _maps(ctx, dcat, g, "fp32c", D=D)
+    keep = np.abs(m64["mu"]) <= 100
+    errs = {k: rel_errors(m32[k], m64[k], keep) for k in m32}
+    print(seed, nc, ng, f"D={D:.2f}", "max errors", {k: f"{v:.2e}" for k, v in errs.items()},
+          "|mu|>100 pixels", int((~keep).sum()))
+    for k, e in errs.items():
+        assert e <= TOL32, (k, e)
