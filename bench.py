@@ -60,7 +60,7 @@ FLOPS_PER_PAIR = 182 + 760
 # says whether the timed build is that one.
 KERNEL_SOURCES = ("lt_eval.cuh", "lt_profiles32.cuh", "lt_profiles64.cuh", "lt_bulk.cuh", "lt_grid32.cu",
                   "lt_grid.cuh", "lt_halo.h", "lt_pack.h")
-INST_SOURCES_SHA = "7518cb9f271e825f"
+INST_SOURCES_SHA = "8e3ea4f58e55c5d4"
 INST_PER_PAIR_FP32C_LENS = 150.6
 FP32_FLOPS_PER_PAIR_FP32C_LENS = 126.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu

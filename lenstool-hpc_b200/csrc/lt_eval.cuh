@@ -47,26 +47,32 @@ __device__ __forceinline__ void eval_chunk64(const lt_rec64 *recs, int count, co
     }
 }
 
-/* The FP64 recomputation's sums: the closed-form Hessian (nie_hess64) of one chunk of
- * lt_nie64 records at Q pixels of arbitrary positions (px[k], py[k]), added to
- * (hxx, hyy, hxy)[k].  The Q pixels' dependent chains are independent of one another, so
- * the compiler interleaves them; nie_hess64's pinned rounding keeps each pair's value the
+/* The FP64 recomputation's sums: convergence and sky-frame shear from the closed form
+ * (nie_kg64) of one chunk of lt_nie64 records at Q pixels of arbitrary positions
+ * (px[k], py[k]), added to (kap, g1, g2)[k] (by one fused multiply-add with the record's
+ * weight for a Kmap).  The Q pixels' dependent chains are independent of one another, so
+ * the compiler interleaves them; nie_kg64's pinned rounding keeps each pair's value the
  * same for any Q and in every kernel. */
 template <int Q, int TYPE>
 __device__ __forceinline__ void eval_nie_q(const lt_nie64 *recs, int count, const double (&px)[Q],
-                                           const double (&py)[Q], int kmap, double (&hxx)[Q], double (&hyy)[Q],
-                                           double (&hxy)[Q])
+                                           const double (&py)[Q], int kmap, double (&kap)[Q], double (&g1)[Q],
+                                           double (&g2)[Q])
 {
 #pragma unroll 1
     for (int h = 0; h < count; h++) {
         const lt_nie64 &r = recs[h];
-        const double w = kmap ? r.w : 1.0;
 #pragma unroll
         for (int k = 0; k < Q; k++) {
-            const Hess64 t = nie_hess64<TYPE>(r, px[k], py[k], w);
-            hxx[k] = __dadd_rn(hxx[k], t.xx);
-            hyy[k] = __dadd_rn(hyy[k], t.yy);
-            hxy[k] = __dadd_rn(hxy[k], t.xy);
+            const Kg64 t = nie_kg64<TYPE>(r, px[k], py[k]);
+            if (kmap) {
+                kap[k] = __fma_rn(r.w, t.k, kap[k]);
+                g1[k] = __fma_rn(r.w, t.g1, g1[k]);
+                g2[k] = __fma_rn(r.w, t.g2, g2[k]);
+            } else {
+                kap[k] = __dadd_rn(kap[k], t.k);
+                g1[k] = __dadd_rn(g1[k], t.g1);
+                g2[k] = __dadd_rn(g2[k], t.g2);
+            }
         }
     }
 }
@@ -74,15 +80,23 @@ __device__ __forceinline__ void eval_nie_q(const lt_nie64 *recs, int count, cons
 /* eval_nie_q over one staged chunk of any profile type. */
 template <int Q>
 __device__ __forceinline__ void eval_nie_chunk(const lt_chunk &c, const lt_nie64 *recs, const double (&px)[Q],
-                                               const double (&py)[Q], int kmap, double (&hxx)[Q],
-                                               double (&hyy)[Q], double (&hxy)[Q])
+                                               const double (&py)[Q], int kmap, double (&kap)[Q], double (&g1)[Q],
+                                               double (&g2)[Q])
 {
     switch (c.type) {
-    case 81: eval_nie_q<Q, 81>(recs, c.count, px, py, kmap, hxx, hyy, hxy); break;
-    case 8: eval_nie_q<Q, 8>(recs, c.count, px, py, kmap, hxx, hyy, hxy); break;
-    case 5: eval_nie_q<Q, 5>(recs, c.count, px, py, kmap, hxx, hyy, hxy); break;
+    case 81: eval_nie_q<Q, 81>(recs, c.count, px, py, kmap, kap, g1, g2); break;
+    case 8: eval_nie_q<Q, 8>(recs, c.count, px, py, kmap, kap, g1, g2); break;
+    case 5: eval_nie_q<Q, 5>(recs, c.count, px, py, kmap, kap, g1, g2); break;
     default: break;
     }
+}
+
+/* The recomputed pixel's Hessian from its convergence and shear sums. */
+__device__ __forceinline__ void nie_hessian(double kap, double g1, double g2, double &hxx, double &hyy, double &hxy)
+{
+    hxx = __dadd_rn(kap, g1);
+    hyy = __dsub_rn(kap, g1);
+    hxy = g2;
 }
 
 /* End of a run of the reference's dispatch (src/gradient2.cpp:240-251): the run's sum

@@ -22,7 +22,7 @@ enum {
  * OP_GRAD takes the dPIE deflection as log(1 + eps) (LT_FP64_FAST; FP32C's FP64 terms
  * always do), OP_GRAD alone in the reference's two-logarithm form (LT_FP64, the queue's
  * exact tiles, the chi2 points); OP_NI with OP_HESS takes the Hessian from the FP64
- * closed-form records lt_nie64 (nie_hess64: the FP32C path's FP64 recomputation) */
+ * closed-form records lt_nie64 (nie_kg64: the FP32C path's FP64 recomputation) */
 enum { OP_GRAD = 1, OP_HESS = 2, OP_POT = 4, OP_HEX = 8, OP_PEX = 16, OP_GFX = 32, OP_NI = 64 };
 
 /* chunk.pad bits: FP32 records (FP32C list), last chunk of a run */

@@ -122,7 +122,8 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
         const lt_chunk c = a.chunks[ci];
         const lt_rec64 *recs = b ? buf1 : buf0;
         if (LIST) {
-            /* the staged records are the closed-form records lt_nie64 */
+            /* the staged records are the closed-form records lt_nie64; acc.hxx, acc.hyy and
+             * acc.hxy hold the convergence and shear sums */
             eval_nie_chunk<P>(c, reinterpret_cast<const lt_nie64 *>(recs), px, lpy, a.kmap, acc.hxx, acc.hyy,
                               acc.hxy);
             if (ci == a.nchunks - 1) {
@@ -130,9 +131,10 @@ __global__ void __launch_bounds__(kThreads, MINB) grid64_kernel(const GridArgs a
                 for (int k = 0; k < P; k++) {
                     if (ly[k] >= a.ny) continue;
                     const long pix = (long)ly[k] * a.nx + lx[k];
+                    double hxx, hyy, hxy;
+                    nie_hessian(acc.hxx[k], acc.hyy[k], acc.hxy[k], hxx, hyy, hxy);
                     for (int o = 0; o < a.nout; o++)
-                        a.out[o][pix] = map_value4(a.kinds[o], 0., 0., acc.hxx[k], acc.hyy[k], acc.hxy[k],
-                                                   acc.hxy[k], 0., a.D, a.mult, a.scale);
+                        a.out[o][pix] = map_value4(a.kinds[o], 0., 0., hxx, hyy, hxy, hxy, 0., a.D, a.mult, a.scale);
                 }
             }
             __syncthreads(); /* buffer b is refilled by the copy issued at step s + 1 */

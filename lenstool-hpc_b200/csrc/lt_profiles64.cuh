@@ -541,15 +541,19 @@ __device__ __forceinline__ void hess_pair(const lt_rec64 &h, double px, double p
 }
 } // namespace ex
 
-/* The sky-frame Hessian of one pair from the real-valued closed form (lt_profiles32.cuh's
- * forms in FP64, record lt_nie64), weight w included: the FP32C path's recomputation of
+/* Convergence and sky-frame shear of one pair, unweighted, from the real-valued closed form
+ * (lt_profiles32.cuh's forms in FP64, record lt_nie64): the FP32C path's recomputation of
  * pixels near critical curves.  About 70 FP64 operations for a dPIE pair against ~95 for
  * the reference's quotient form, and no 0/0 point; equal to it within ~1e-15 of the terms.
  * Every operation's rounding is pinned (explicit round-to-nearest multiply, add and fused
  * multiply-add), so the function can be inlined into any kernel, and interleaved over
  * several pixels, and still round each pair alike everywhere. */
+struct Kg64 {
+    double k, g1, g2;
+};
+
 template <int TYPE>
-__device__ __forceinline__ Hess64 nie_hess64(const lt_nie64 &h, double px, double py, double w)
+__device__ __forceinline__ Kg64 nie_kg64(const lt_nie64 &h, double px, double py)
 {
     using ex::A;
     using ex::M;
@@ -589,8 +593,7 @@ __device__ __forceinline__ Hess64 nie_hess64(const lt_nie64 &h, double px, doubl
             g2 = M(-2., M(uv, dEK));
         }
     }
-    const double gs1 = __fma_rn(g1, h.c2t, -M(g2, h.s2t)), gs2 = __fma_rn(g1, h.s2t, M(g2, h.c2t));
-    return {M(w, A(k, gs1)), M(w, S(k, gs1)), M(w, gs2)};
+    return {k, __fma_rn(g1, h.c2t, -M(g2, h.s2t)), __fma_rn(g1, h.s2t, M(g2, h.c2t))};
 }
 
 /* The FP64 terms of one pair as out-of-line functions, for the FP32C path's FP64 work (its

@@ -294,7 +294,7 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
     if (threadIdx.x == 0 && status) atomicAdd(reinterpret_cast<unsigned long long *>(status + 2), (unsigned long long)n);
     bool have[P];
     int qx[P], qy[P];
-    double qpx[P], qpy[P], hxx[P], hyy[P], hxy[P];
+    double qpx[P], qpy[P], kap[P], g1[P], g2[P];
 #pragma unroll
     for (int k = 0; k < P; k++) {
         const int e = k * kQThreads + (int)threadIdx.x;
@@ -304,23 +304,25 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
         qy[k] = tile_y0 + l / (32 * P);
         qpx[k] = pixel_x(a, qx[k]);
         qpy[k] = pixel_y(a, qy[k]);
-        hxx[k] = hyy[k] = hxy[k] = 0.;
+        kap[k] = g1[k] = g2[k] = 0.;
     }
     const bool ok2 = walk_chunks(st, a.chunks, a.nchunks, reinterpret_cast<const lt_rec64 *>(it.nie64), nullptr,
                                  status, [&](const lt_chunk &c, const unsigned char *buf) {
                                      if (!have[0]) return;
                                      eval_nie_chunk<P>(c, reinterpret_cast<const lt_nie64 *>(buf), qpx, qpy, a.kmap,
-                                                       hxx, hyy, hxy);
+                                                       kap, g1, g2);
                                  });
     if (!ok2) return false;
 #pragma unroll
     for (int k = 0; k < P; k++) {
         if (!have[k]) continue;
         const long p = (long)qy[k] * a.nx + qx[k];
+        double hxx, hyy, hxy;
+        nie_hessian(kap[k], g1[k], g2[k], hxx, hyy, hxy);
         for (int o = 0; o < a.nout; o++) {
             const int kind = a.kinds[o];
             if (is_grad_kind(kind) || kind == KIND_POT) continue;
-            a.out[o][p] = map_value(kind, 0., 0., hxx[k], hyy[k], hxy[k], 0., a.D, a.mult, a.scale);
+            a.out[o][p] = map_value(kind, 0., 0., hxx, hyy, hxy, 0., a.D, a.mult, a.scale);
         }
     }
     return true;
