@@ -91,6 +91,8 @@ def _single(ctx, cat, g, kinds, kw, precision, D=0.6, scale=1.3):
 @pytest.mark.parametrize("precision", ["fp32c", "fp64"])
 def test_batch_equals_single_calls(ctx, precision):
     import torch
+    ctx.synchronize()
+    ctx.recompute_count()  # count from here on
     reqs, planes, expect = [], [], []
     for cat, g, kinds, kw in _requests():
         h = ctx.upload(cat)
@@ -100,11 +102,17 @@ def test_batch_equals_single_calls(ctx, precision):
         expect.append(_single(ctx, h, g, kinds, kw, precision))
     b = ctx.batch(reqs, precision=precision)
     assert len(b) == len(reqs)
+    ctx.synchronize()
+    single_recomputed = ctx.recompute_count()
     n0 = lt.launch_count()
     b.launch()
     ctx.synchronize()
     torch.cuda.synchronize()
     assert lt.launch_count() - n0 == 2  # queue reset + persistent kernel
+    # the batch recomputes in FP64 exactly the pixels the single calls recomputed
+    assert ctx.recompute_count() == single_recomputed
+    if precision == "fp32c":
+        assert single_recomputed > 0
     for i, (outs, exp) in enumerate(zip(planes, expect)):
         for k, o in outs.items():
             got = o.cpu().numpy()
