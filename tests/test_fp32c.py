@@ -269,3 +269,28 @@ def test_fp32c_random_fields_hold_the_bound(ctx, seed):
           "|mu|>100 pixels", int((~keep).sum()))
     for k, e in errs.items():
         assert e <= TOL32, (k, e)
+
+
+@pytest.mark.parametrize("nx,ny", [(1, 1), (1, 37), (41, 1), (3, 5), (65, 9), (130, 17)])
+def test_fp32c_degenerate_grids(ctx, nx, ny):
+    """Grids smaller than a tile or a warp's pixel box in either direction, with partial
+    tiles at both edges: every map within the bound of LT_FP64 (the kernels clamp the
+    pixels beyond the grid and store none of them), host and device outputs alike."""
+    import torch
+    cat = catalog.cluster_galaxy_catalog(2, 150, 77)
+    g = catalog.Grid(-37.3, 25.1, -12.7, 31.9, nx, ny, dx=62.4 / max(nx - 1, 1), dy=44.6 / max(ny - 1, 1))
+    dcat = ctx.upload(cat)
+    kinds = ("kappa", "gamma1", "gamma2", "mu")
+    m64 = _maps(ctx, dcat, g, "fp64", kinds=kinds)
+    m32 = _maps(ctx, dcat, g, "fp32c", kinds=kinds)
+    keep = np.abs(m64["mu"]) <= 100
+    for k in kinds:
+        assert m32[k].shape == (ny, nx)
+        if keep.any():
+            assert rel_errors(m32[k], m64[k], keep) <= TOL32, k
+    host = ctx.lens_maps(dcat, g, precision="fp32c", dlsds=0.6)
+    dev = {k: torch.empty((ny, nx), dtype=torch.float64, device="cuda") for k in host}
+    ctx.lens_maps(dcat, g, precision="fp32c", dlsds=0.6, out=dev)
+    ctx.synchronize()
+    for k in host:
+        assert np.array_equal(host[k], dev[k].cpu().numpy()), k
