@@ -286,7 +286,8 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
     if (!recompute) return true;
     __syncthreads();
     /* the flagged pixels (at most the tile's 32 P x 8 = P kQThreads): P a thread, in one
-     * walk of the catalogue's FP64 closed-form records */
+     * walk of the catalogue's FP64 closed-form records; one a thread when they are at most
+     * kQThreads (a second, empty pixel would double the walk's work) */
     const int n = *s_count;
     const int tile_x0 = (tile % a.tiles_x) * 32 * P, tile_y0 = (tile / a.tiles_x) * 8;
     if (n == 0) return true;
@@ -306,13 +307,23 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
         qpy[k] = pixel_y(a, qy[k]);
         kap[k] = g1[k] = g2[k] = 0.;
     }
+    const bool one = n <= kQThreads; /* block-uniform */
+    double px1[1] = {qpx[0]}, py1[1] = {qpy[0]}, kap1[1] = {0.}, g11[1] = {0.}, g21[1] = {0.};
     const bool ok2 = walk_chunks(st, a.chunks, a.nchunks, reinterpret_cast<const lt_rec64 *>(it.nie64), nullptr,
                                  status, [&](const lt_chunk &c, const unsigned char *buf) {
                                      if (!have[0]) return;
-                                     eval_nie_chunk<P>(c, reinterpret_cast<const lt_nie64 *>(buf), qpx, qpy, a.kmap,
-                                                       kap, g1, g2);
+                                     const lt_nie64 *recs = reinterpret_cast<const lt_nie64 *>(buf);
+                                     if (one)
+                                         eval_nie_chunk<1>(c, recs, px1, py1, a.kmap, kap1, g11, g21);
+                                     else
+                                         eval_nie_chunk<P>(c, recs, qpx, qpy, a.kmap, kap, g1, g2);
                                  });
     if (!ok2) return false;
+    if (one) {
+        kap[0] = kap1[0];
+        g1[0] = g11[0];
+        g2[0] = g21[0];
+    }
 #pragma unroll
     for (int k = 0; k < P; k++) {
         if (!have[k]) continue;
