@@ -285,9 +285,10 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
     }
     if (!recompute) return true;
     __syncthreads();
-    /* the flagged pixels (at most the tile's 32 P x 8 = P kQThreads): P a thread, in one
-     * walk of the catalogue's FP64 closed-form records; one a thread when they are at most
-     * kQThreads (a second, empty pixel would double the walk's work) */
+    /* the flagged pixels (at most the tile's 32 P x 8 = P kQThreads), in one walk of the
+     * catalogue's FP64 closed-form records: thread t takes entries t and t + kQThreads; a warp
+     * with no second entry evaluates one pixel a thread (an empty second pixel would double
+     * its work) */
     const int n = *s_count;
     const int tile_x0 = (tile % a.tiles_x) * 32 * P, tile_y0 = (tile / a.tiles_x) * 8;
     if (n == 0) return true;
@@ -307,7 +308,7 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
         qpy[k] = pixel_y(a, qy[k]);
         kap[k] = g1[k] = g2[k] = 0.;
     }
-    const bool one = n <= kQThreads; /* block-uniform */
+    const bool one = !__any_sync(0xffffffffu, P == 2 && have[P - 1]); /* warp-uniform */
     double px1[1] = {qpx[0]}, py1[1] = {qpy[0]}, kap1[1] = {0.}, g11[1] = {0.}, g21[1] = {0.};
     const bool ok2 = walk_chunks(st, a.chunks, a.nchunks, reinterpret_cast<const lt_rec64 *>(it.nie64), nullptr,
                                  status, [&](const lt_chunk &c, const unsigned char *buf) {
