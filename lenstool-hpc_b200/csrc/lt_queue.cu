@@ -293,7 +293,8 @@ __device__ __noinline__ bool tile32(const QItem &it, int tile, Stage &st, int32_
     const int tile_x0 = (tile % a.tiles_x) * 32 * P, tile_y0 = (tile / a.tiles_x) * 8;
     if (n == 0) return true;
     /* the count of recomputed pixels (lt_recompute_count): word 2 of the status block */
-    if (threadIdx.x == 0 && status) atomicAdd(reinterpret_cast<unsigned long long *>(status + 2), (unsigned long long)n);
+    if (threadIdx.x == 0 && status)
+        atomicAdd(reinterpret_cast<unsigned long long *>(status + 2), (unsigned long long)n);
     bool have[P];
     int qx[P], qy[P];
     double qpx[P], qpy[P], kap[P], g1[P], g2[P];
