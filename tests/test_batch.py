@@ -40,7 +40,7 @@ def _dev(g):
 
 def _requests(seed=7):
     """Mixed requests: perturbed cluster catalogues, PIEMD/SIS variants, odd and even grids,
-    Hessian maps, potential, deflection and a Kmap mass map."""
+    Hessian maps, potential, deflection and Kmap mass and magnification maps."""
     rng = np.random.Generator(np.random.PCG64(seed))
     base = catalog.cluster_galaxy_catalog(2, 198, 20261203)
     cats = [catalog.perturb_catalog(base, rng) for _ in range(3)]
@@ -57,7 +57,7 @@ def _requests(seed=7):
         (["kappa", "gamma1", "gamma2", "mu", "potential"], {}),
         (["deflection_x", "deflection_y", "ampli1"], {}),
         (["shear2", "ampli3", "hess_a", "hess_d"], {}),
-        (["mass"], {"kmap": True, "mult": 0.37}),
+        (["mass", "mu"], {"kmap": True, "mult": 0.37}),
     ]
     out = []
     for cat, g, (kinds, kw) in zip(cats, grids, specs):
