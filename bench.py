@@ -65,7 +65,7 @@ INST_PER_PAIR_FP32C_LENS = 150.6
 FP32_FLOPS_PER_PAIR_FP32C_LENS = 126.4
 # DRAM bytes (read + write) of one launch of that kernel at 4096^2, from a single-pass ncu
 # capture of this bench's own launch (summary under profiles/)
-TRAFFIC_FP32C_LENS_4096 = 16228864 + 633445888
+TRAFFIC_FP32C_LENS_4096 = 14311424 + 630767872
 
 
 def _package():
